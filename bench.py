@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""bench.py — FBP voxel-angle updates/s of the B200 backend (one JSON line).
+
+Workload (default, "large"): a 512^3 float32 phantom of 32 seeded random
+ellipsoids (rotated, summed inside the unit sphere), 720 angles on [0, pi),
+Nd = ceil(sqrt(2) 512) rounded up to odd = 725 detector bins, Shepp-Logan
+filter. One step = the whole reconstructVolume path on the device: per-slice
+statistics, forward projection of all 512 slices, ramp filtering, backprojection
+and denormalisation. updates = N^2 * slices * angles per volume. Synthetic
+data (no dataset involved); the volume (0.54 GB) exceeds the 126 MB L2, so no
+flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--config small|large|precision]
+
+N > 1 runs under torch.distributed.run, one rank per GPU, each rank
+reconstructing its own volume (weak scaling; no data-path collective).
+--impl reference times the reference's own CPU implementation of the path
+(OpenMPBackend built from its sources, oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "small": dict(n=128, nz=128, na=180, ellipsoids=10, filter=0, seed=1,
+                  name="128^3 phantom (10 ellipsoids), 180 angles, Ram-Lak"),
+    "large": dict(n=512, nz=512, na=720, ellipsoids=32, filter=1, seed=2,
+                  name="512^3 phantom (32 ellipsoids), 720 angles, Shepp-Logan"),
+    "precision": dict(n=1024, nz=256, na=1440, ellipsoids=64, filter=4, seed=3,
+                      name="1024^2 x 256 phantom (64 ellipsoids), 1440 angles, Hann"),
+}
+FILTER_NAMES = ["ramlak", "shepp-logan", "hamming", "cosine", "hann", "bartlett"]
+METRIC = "FBP voxel-angle updates/s"
+UNIT = "updates/s"
+
+
+def odd_nd(n: int) -> int:
+    nd = math.ceil(math.sqrt(2.0) * n)
+    return nd + 1 if nd % 2 == 0 else nd
+
+
+def circle_voxels(n: int) -> int:
+    """Voxels the reference reconstructs: xx^2 + yy^2 <= r^2 with r = n//2."""
+    r = n // 2
+    c = 0
+    for y in range(n):
+        yy = y - r
+        rem = r * r - yy * yy
+        if rem < 0:
+            continue
+        s = math.isqrt(rem)
+        c += max(0, min(n - 1, r + s) - max(0, r - s) + 1)
+    return c
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str, period_ms: int = 100):
+        self.rows = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", gpu_id, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", str(period_ms)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        if not self.rows:
+            return None
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in self.rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in self.rows if num(r[2]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def gpu_id_for(device: int) -> str:
+    import torch
+    try:
+        u = str(torch.cuda.get_device_properties(device).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        return vis.split(",")[device] if vis else str(device)
+
+
+def load_profile_traffic(config: str):
+    """DRAM bytes per backprojection launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"backproject_{config}_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+# ------------------------------------------------------------- CPU baseline
+def cpu_reference_rate(cfg: dict, slices: int, params, repeats: int = 1):
+    """The reference's OpenMPBackend per-slice path (computeSinogram with the
+    config's odd detector + reconstructSlice) on `slices` slices of the
+    phantom, all host threads. Returns (updates/s, threads, kind, isa)."""
+    import numpy as np
+
+    import oracle as O
+    from oracle import reference as R
+    n, nz, na, kind = cfg["n"], cfg["nz"], cfg["na"], cfg["filter"]
+    nd = odd_nd(n)
+    z0 = nz // 2 - slices // 2
+    vol = O.phantom_sum_slab(params, n, n, nz, z0, slices)
+    lib, isa = R.timing_lib()
+    if lib is None:
+        # reference not built: the float restatement of SerialBackend (1 thread)
+        t0 = time.perf_counter()
+        for z in range(slices):
+            s, a, mm = O.sinogram_f32(vol[z], na, nd)
+            O.reconstruct_slice_f32(s, a, n, kind)
+        dt = time.perf_counter() - t0
+        return n * n * slices * na / dt, 1, "port", "x86-64", f"{slices} slices (SerialBackend restatement)"
+    threads = os.cpu_count() or 1
+    lib.ref_set_threads(threads)
+    # warm-up on one slice
+    s, a, mm = R.compute_sinogram(R.OPENMP, vol[0], na, nd, lib=lib)
+    R.reconstruct_slice(R.OPENMP, s, a, n, kind, mm[0], mm[1], lib=lib)
+    best = None
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        for z in range(slices):
+            s, a, mm = R.compute_sinogram(R.OPENMP, vol[z], na, nd, lib=lib)
+            R.reconstruct_slice(R.OPENMP, s, a, n, kind, mm[0], mm[1], lib=lib)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    sample = f"{slices} of {nz} slices, OpenMPBackend computeSinogram(nd={nd}) + reconstructSlice, {isa}"
+    return n * n * slices * na / best, threads, "reference", isa, sample
+
+
+def run_reference(args, cfg, rank: int, world: int):
+    """--impl reference: the reference's CPU path, rank 0 only."""
+    if rank != 0:
+        return 0
+    import qtctreconstruction_b200 as ctb  # host-side parameter generation only (no GPU)
+    params = ctb.phantom_params(cfg["seed"], cfg["ellipsoids"])
+    n, nz, na = cfg["n"], cfg["nz"], cfg["na"]
+    slices = args.ref_slices
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        cpu_reference_rate(cfg, 1, params)
+    rates = []
+    threads, kind, isa, sample = 1, "port", "", ""
+    for _ in range(args.steps):
+        r, threads, kind, isa, sample = cpu_reference_rate(cfg, slices, params)
+        rates.append(r)
+    value = statistics.median(rates)
+    step_ms = n * n * slices * na / value * 1e3
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": args.config, "description": cfg["name"], "n": n, "slices": nz,
+                   "angles": na, "detector_bins": odd_nd(n), "filter": FILTER_NAMES[cfg["filter"]],
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------- ours
+def run_ours(args, cfg, rank: int, world: int, local: int):
+    import numpy as np
+    import torch
+
+    import qtctreconstruction_b200 as ctb
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device(f"cuda:{local}"))
+    n, nz, na, kind = cfg["n"], cfg["nz"], cfg["na"], cfg["filter"]
+    nd = odd_nd(n)
+    updates = n * n * nz * na
+    be = ctb.B200Backend(local)
+    stream = torch.cuda.current_stream()
+    be.set_stream(stream.cuda_stream)
+    be.set_profiling(True)
+
+    params = ctb.phantom_params(cfg["seed"], cfg["ellipsoids"])
+    vol = torch.empty((nz, n, n), dtype=torch.float32, device="cuda")
+    out = torch.empty_like(vol)
+    be.phantom_d(params, n, n, nz, vol.data_ptr())
+
+    def step():
+        be.reconstruct_volume_d(vol.data_ptr(), n, nz, na, nd, kind, out.data_ptr())
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timing
+    sampler = ClockSampler(gpu_id_for(local))
+    barrier()
+    l0 = be.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = be.launch_count() - l0
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    stages = np.mean([be.stage_times(back) for back in range(args.steps)], axis=0)
+
+    # ---- end to end through the host-buffer C ABI call (pinned host buffers)
+    hin = torch.empty((nz, n, n), dtype=torch.float32, pin_memory=True)
+    hin.copy_(vol.cpu())
+    hout = torch.empty_like(hin, pin_memory=True)
+    vol_host_ptr, out_host_ptr = hin.data_ptr(), hout.data_ptr()
+
+    def e2e_step():
+        be.reconstruct_volume_host(vol_host_ptr, n, nz, na, nd, kind, out_host_ptr)
+
+    e2e_step()
+    barrier()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(3, args.steps // 4)
+    e2.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e2.elapsed_time(e3) / e2e_steps
+
+    # max over ranks
+    if dist is not None:
+        t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+
+    if rank == 0:
+        value = world * updates / (ms * 1e-3)
+        smem_gbs = be.probe_smem_bandwidth()
+        inside = circle_voxels(n) * nz * na
+        bp_ms = float(stages[3])
+        achieved = inside * 8.0 / (bp_ms * 1e-3) / 1e9  # two float taps per in-circle update
+        peaks = measured_peaks()
+        hbm_peak = peaks.get("hbm_gbs")
+        sq = math.ceil(math.sqrt(2.0) * nd)
+        filt_bytes = 4.0 * (nd + sq) * nz * na
+        traffic = load_profile_traffic(args.config)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.config, "description": cfg["name"], "n": n, "slices": nz,
+                       "angles": na, "detector_bins": nd, "filter": FILTER_NAMES[kind],
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 gpu",
+                       "l2": "inputs larger than L2 (volume 0.54 GB per step), no flush"
+                       if n * n * nz * 4 > 126e6 else "inputs smaller than L2"},
+            "gpu_launches": launches,
+            "stage_ms": {"stats_normalize": stages[0], "forward": stages[1], "filter": stages[2],
+                         "backproject": stages[3]},
+            "fbp_only": {"value": updates / ((stages[2] + stages[3]) * 1e-3), "unit": UNIT,
+                         "note": "filter + backprojection kernels only"},
+            "roofline": {"kernel": "k_backproject", "bound": "smem", "achieved": achieved,
+                         "peak": smem_gbs, "unit": "GB/s", "frac": achieved / smem_gbs,
+                         "traffic": traffic,
+                         "peak_source": "measured shared-memory load bandwidth (probe kernel, same run)",
+                         "algorithmic": "8 B (two float taps) per in-circle voxel-angle update"},
+            "roofline_filter": {"kernel": "k_filter", "bound": "hbm",
+                                "achieved": filt_bytes / (stages[2] * 1e-3) / 1e9,
+                                "peak": hbm_peak, "unit": "GB/s",
+                                "frac": (filt_bytes / (stages[2] * 1e-3) / 1e9 / hbm_peak) if hbm_peak else None,
+                                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_peak else None},
+            "e2e": {"value": world * updates / (e2e_ms * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": 4 * n * n * nz, "d2h_bytes_per_step": 4 * n * n * nz,
+                    "ms_per_step": e2e_ms, "api": "ctb_reconstruct_volume (pinned host buffers)"},
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            r, threads, kind_b, isa, sample = cpu_reference_rate(cfg, args.ref_slices, params)
+            line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": threads, "kind": kind_b,
+                                    "sample": sample}
+        print(json.dumps(line), flush=True)
+    be.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="large")
+    ap.add_argument("--ref-slices", type=int, default=2, help="slices per CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        return run_reference(args, cfg, rank, world)
+    return run_ours(args, cfg, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,206 @@
+/*
+ * ctb200.h — C ABI of libctb200.so, the B200 (sm_100a) backend for
+ * QtCTReconstruction's parallel-beam FBP path.
+ *
+ * Every entry point uses plain pointers, sizes and integer status codes: no C++
+ * or torch types cross this boundary and no exception escapes it. Host
+ * pointers are caller-owned; device workspaces are owned by the context.
+ * A context serialises its own calls with an internal mutex, so one context
+ * may be shared by threads (the reference controller calls computeSinogram
+ * from an OpenMP loop, CtReconstructionController.cpp:1232-1242).
+ *
+ * Conventions follow the reference's SerialBackend (the oracle):
+ *   slice        [y][x] row-major float, width x height   (CTTypes.h:15-74)
+ *   volume       [z][y][x] float                          (CTTypes.h:101)
+ *   sinogram     [angle][bin] float, na rows of nd bins   (SerialBackend.cpp:82-83)
+ *   sinograms    [z][angle][bin]  (the consumer volume (nz, na, bins))
+ *   angles       degrees, float; uniform angles are 180/na * a in float
+ *   filter ids   ReconstructionParams::FilterType order   (CTTypes.h:151)
+ *
+ * Citations name files of the QtCTReconstruction project.
+ */
+#ifndef CTB200_H
+#define CTB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ctb_ctx ctb_ctx;
+
+typedef enum ctb_status {
+    CTB_OK = 0,
+    CTB_ERR_INVALID = 1,      /* bad sizes or null pointers (reference: empty result) */
+    CTB_ERR_CUDA = 2,         /* a CUDA runtime call failed; see ctb_last_error */
+    CTB_ERR_OOM = 3,          /* device allocation failed or budget exceeded */
+    CTB_ERR_UNSUPPORTED = 4,  /* size outside what the kernels support */
+    CTB_ERR_NO_DEVICE = 5,    /* no usable sm_100 device */
+    CTB_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up */
+    CTB_ERR_CANCELLED = 7,    /* serving: request cancelled */
+    CTB_ERR_NOT_FOUND = 8,    /* serving: unknown request id */
+    CTB_ERR_BUSY = 9          /* serving: request still running */
+} ctb_status;
+
+/* ReconstructionParams::FilterType (CTTypes.h:151). */
+typedef enum ctb_filter {
+    CTB_FILTER_RAMP = 0,
+    CTB_FILTER_SHEPP_LOGAN = 1,
+    CTB_FILTER_HAMMING = 2,
+    CTB_FILTER_COSINE = 3,
+    CTB_FILTER_HANN = 4,
+    CTB_FILTER_BARTLETT = 5
+} ctb_filter;
+
+/* Output units of a reconstruction from sinograms.
+ *   NONE    normalised units, as SerialBackend::reconstructSlice returns them
+ *           (SerialBackend.cpp:142-255) and as the interface's default
+ *           reconstructVolumeFromSinograms stores them (BackendFactory.cpp:17-60);
+ *   SERIAL  out * (span <= 0 ? 1 : span) + min   (SerialBackend.cpp:297-304);
+ *   OPENMP  out * span + min, or min everywhere when span <= 0
+ *           (OpenMPBackend.cpp:37-59).
+ * min/span come from the per-slice stats (see ctb_forward_d). */
+typedef enum ctb_denorm {
+    CTB_DENORM_NONE = 0,
+    CTB_DENORM_SERIAL = 1,
+    CTB_DENORM_OPENMP = 2
+} ctb_denorm;
+
+/* ---------------------------------------------------------------- lifecycle */
+
+/* Create a context on CUDA device `device`. Replaces the construction done by
+ * BackendFactory::create (BackendFactory.cpp:62-82); CTB_ERR_NO_DEVICE is the
+ * isAvailable() == false case (IReconstructionBackend.h:18). */
+ctb_status ctb_create(ctb_ctx** out, int device);
+void ctb_destroy(ctb_ctx* ctx);
+/* Message of the last failure on this context ("" if none). */
+const char* ctb_last_error(const ctb_ctx* ctx);
+const char* ctb_status_string(ctb_status s);
+/* Run subsequent device work on `stream` (a cudaStream_t; NULL = the
+ * context's own stream). */
+ctb_status ctb_set_stream(ctb_ctx* ctx, void* stream);
+/* Block until all work issued by the context has finished. */
+ctb_status ctb_synchronize(ctb_ctx* ctx);
+/* IReconstructionBackend::lastSinogramTimeMs / lastReconstructionTimeMs
+ * (IReconstructionBackend.h:50-54): device time of the last forward and
+ * filter+backprojection stages, measured with CUDA events. */
+double ctb_last_sinogram_ms(const ctb_ctx* ctx);
+double ctb_last_reconstruction_ms(const ctb_ctx* ctx);
+/* Number of kernel launches the context has issued so far. */
+uint64_t ctb_launch_count(const ctb_ctx* ctx);
+
+/* Per-stage device timing. With profiling on, every volume reconstruction
+ * (ctb_reconstruct_volume[_d]) records CUDA events between its stages into a
+ * ring of 256 entries. ctb_stage_times(ctx, back, ms) reads the entry `back`
+ * calls ago (0 = latest; waits for it) into ms[0..3] = {statistics +
+ * normalisation, forward projection, filtering, backprojection}. */
+ctb_status ctb_set_profiling(ctb_ctx* ctx, int enable);
+ctb_status ctb_stage_times(ctb_ctx* ctx, int back, double* ms);
+
+/* Measured shared-memory load bandwidth of this GPU in GB/s: a conflict-free
+ * 16-byte-per-lane load loop over all SMs, timed with CUDA events. The
+ * backprojector's roofline denominator. */
+ctb_status ctb_probe_smem_bandwidth(ctb_ctx* ctx, double* gbs);
+
+/* Geometry helpers shared with the reference (SerialBackend.cpp:152-163):
+ * square_bins = ceil(sqrt(2)*bins), pad_before = square_bins/2 - bins/2,
+ * fft_size = max(64, nextPow2(2*square_bins)). */
+ctb_status ctb_pad_geometry(int bins, int* square_bins, int* pad_before, int* fft_size);
+/* FilterDesign::createFilter (FilterDesign.cpp:13-111), evaluated in double
+ * precision and rounded to float: fft_size/2+1 values. */
+ctb_status ctb_filter_response(int fft_size, int filter, float* H);
+
+/* ------------------------------------------- host-buffer entry points
+ * These mirror IReconstructionBackend (IReconstructionBackend.h:10-55); the
+ * B200Backend C++ class forwards to them. Host<->device copies are inside. */
+
+/* IReconstructionBackend::computeSinogram (SerialBackend.cpp:59-136).
+ * sino_out: num_angles x detector_bins. angles_deg_out (num_angles) and
+ * minmax_out {min, max} may be NULL. */
+ctb_status ctb_compute_sinogram(ctb_ctx* ctx, const float* slice, int width, int height,
+                                int num_angles, int detector_bins, float* sino_out,
+                                float* angles_deg_out, float* minmax_out);
+
+/* IReconstructionBackend::reconstructSlice (SerialBackend.cpp:142-255):
+ * normalised units, output_size x output_size. */
+ctb_status ctb_reconstruct_slice(ctb_ctx* ctx, const float* sino, int num_angles,
+                                 int detector_bins, const float* angles_deg, int output_size,
+                                 int filter, float* out);
+
+/* IReconstructionBackend::reconstructVolume (SerialBackend.cpp:261-318):
+ * per slice, forward projection onto detector_bins bins (the reference passes
+ * detector_bins = n), FBP back to n x n and denormalisation with the slice's
+ * min/span. vol and out: depth x n x n. */
+ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int depth,
+                                  int num_angles, int detector_bins, int filter, float* out);
+
+/* IReconstructionBackend::reconstructVolumeFromSinograms
+ * (IReconstructionBackend.h:39-44; default loop BackendFactory.cpp:17-60).
+ * sinos: depth x num_angles x bins; out: depth x bins x bins. The per-slice
+ * min/max used by SERIAL/OPENMP denormalisation are taken from the sinogram
+ * itself, as the reference's default implementation does. */
+ctb_status ctb_reconstruct_from_sinograms(ctb_ctx* ctx, const float* sinos, int depth,
+                                          int num_angles, int bins, const float* angles_deg,
+                                          int filter, int denorm, float* out);
+
+/* ------------------------------------------- device-buffer entry points
+ * Inputs already resident in device memory; work is queued on the context's
+ * stream and the call returns without synchronising. */
+
+/* Forward projection of depth slices (n x n each) to sinograms
+ * d_sino[z][a][detector_bins]. d_stats receives 4 floats per slice:
+ * {min, max, span_fwd, span_denorm} with span_fwd = (max-min < 1e-6 ? 1 : max-min)
+ * (SerialBackend.cpp:78-80) and span_denorm = (max-min <= 0 ? 1 : max-min)
+ * (SerialBackend.cpp:298-300). angles_deg: host array (NULL = uniform). */
+ctb_status ctb_forward_d(ctb_ctx* ctx, const float* d_vol, int n, int depth, int num_angles,
+                         int detector_bins, const float* angles_deg, float* d_sino,
+                         float* d_stats);
+
+/* Ramp filtering + backprojection of d_sino[z][a][bins] into
+ * d_out[z][output_size][output_size]. d_stats (4 floats per slice, as written
+ * by ctb_forward_d) selects the denormalisation; NULL means normalised units. */
+ctb_status ctb_fbp_d(ctb_ctx* ctx, const float* d_sino, int depth, int num_angles, int bins,
+                     const float* angles_deg, int output_size, int filter, const float* d_stats,
+                     int denorm, float* d_out);
+
+/* reconstructVolume on device buffers: forward + filter + backprojection +
+ * Serial denormalisation. */
+ctb_status ctb_reconstruct_volume_d(ctb_ctx* ctx, const float* d_vol, int n, int depth,
+                                    int num_angles, int detector_bins, int filter, float* d_out);
+
+/* ------------------------------------------------------------ phantoms */
+
+/* Summed random-ellipsoid phantom (the benchmark phantom; a new generator mode
+ * beside Generator3D). Records of 16 floats per ellipsoid: centre (3),
+ * rotation rows (9), inverse squared semi-axes (3), density (1); voxel
+ * coordinates (2i-(n-1))/n per axis, zero outside the unit sphere. */
+ctb_status ctb_phantom_params(uint64_t seed, int count, float* params);
+ctb_status ctb_phantom_sum_d(ctb_ctx* ctx, const float* params, int count, int nx, int ny,
+                             int nz, float* d_vol);
+ctb_status ctb_phantom_sum(ctb_ctx* ctx, const float* params, int count, int nx, int ny, int nz,
+                           float* vol);
+
+/* Generator3D::generateBrainHU on the GPU with the CPU generator's random
+ * stream (Generator3DCPU.cpp:35-117): axis-aligned ellipsoids in millimetres,
+ * max-composited over -1000 HU. tissue: soft then bone tissue, 8 floats each
+ * {hu_min, hu_max, size_min_mm, size_max_mm, peripheral_only, r_min, r_max,
+ * probability} (Generator3D.h:16-34). */
+ctb_status ctb_generator3d(ctb_ctx* ctx, int nx, int ny, int nz, float radius_mm, int count,
+                           uint32_t seed, const float* tissue, float* vol);
+
+/* --------------------------------------------------------- point cloud */
+
+/* IReconstructionBackend::extractPointCloud (SerialBackend.cpp:325-346) with
+ * index coordinates: points (x, y, z, hu) with hu > threshold in z, y, x
+ * order. Writes at most `capacity` points; *count receives the total. */
+ctb_status ctb_extract_point_cloud(ctb_ctx* ctx, const float* vol, int nx, int ny, int nz,
+                                   float threshold, float* points, int64_t capacity,
+                                   int64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CTB200_H */

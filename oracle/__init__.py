@@ -79,6 +79,7 @@ def _declare_oracle(L):
     L.orc_reconstruct_volume_f32.argtypes = [_F32P, i, i, i, i, i, _F32P]
     L.orc_reconstruct_volume_f64.argtypes = [_F32P, i, i, i, i, i, _F64P]
     L.orc_phantom_sum.argtypes = [_F32P, i, i, i, i, _F32P]
+    L.orc_phantom_sum_slab.argtypes = [_F32P, i, i, i, i, i, i, _F32P]
     L.orc_generator3d.argtypes = [i, i, i, f, i, ctypes.c_uint, _F32P, _F32P]
     L.orc_point_cloud.argtypes = [_F32P, i, i, i, f, p, ctypes.c_longlong,
                                   ctypes.POINTER(ctypes.c_longlong)]
@@ -212,6 +213,14 @@ def phantom_sum(params: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
     k = p.size // 16
     vol = np.zeros((nz, ny, nx), np.float32)
     _ok(lib().orc_phantom_sum(p, k, nx, ny, nz, vol), "phantom_sum")
+    return vol
+
+
+def phantom_sum_slab(params: np.ndarray, nx: int, ny: int, nz: int, z0: int, nzs: int) -> np.ndarray:
+    """Slices [z0, z0+nzs) of phantom_sum(params, nx, ny, nz)."""
+    p = np.ascontiguousarray(params, np.float32).reshape(-1)
+    vol = np.zeros((nzs, ny, nx), np.float32)
+    _ok(lib().orc_phantom_sum_slab(p, p.size // 16, nx, ny, nz, z0, nzs, vol), "phantom_sum_slab")
     return vol
 
 

@@ -619,9 +619,20 @@ int orc_reconstruct_volume_f64(const float* vol, int n, int nz, int na, int nd, 
 // X = (2x - (nx-1)) / nx (likewise y, z); voxels outside the unit sphere are 0.
 // The arithmetic order is fixed so the device rasteriser can match it bit for bit:
 // every product and sum is rounded to float separately (no fused multiply-add).
+int orc_phantom_sum_slab(const float* params, int k, int nx, int ny, int nz, int z0, int nzs,
+                         float* vol);
 int orc_phantom_sum(const float* params, int k, int nx, int ny, int nz, float* vol) {
-    if (!params || k < 0 || nx <= 0 || ny <= 0 || nz <= 0 || !vol) return 1;
-    for (int z = 0; z < nz; ++z) {
+    return orc_phantom_sum_slab(params, k, nx, ny, nz, 0, nz, vol);
+}
+
+// A slab [z0, z0 + nzs) of the same phantom (coordinates of the full nz grid).
+int orc_phantom_sum_slab(const float* params, int k, int nx, int ny, int nz, int z0, int nzs,
+                         float* vol) {
+    if (!params || k < 0 || nx <= 0 || ny <= 0 || nz <= 0 || z0 < 0 || nzs <= 0 ||
+        z0 + nzs > nz || !vol)
+        return 1;
+    for (int zz = 0; zz < nzs; ++zz) {
+        const int z = z0 + zz;
         const float Z = (2.0f * static_cast<float>(z) - static_cast<float>(nz - 1)) / static_cast<float>(nz);
         for (int y = 0; y < ny; ++y) {
             const float Y = (2.0f * static_cast<float>(y) - static_cast<float>(ny - 1)) / static_cast<float>(ny);
@@ -640,7 +651,7 @@ int orc_phantom_sum(const float* params, int k, int nx, int ny, int nz, float* v
                         if (q <= 1.0f) acc += p[15];
                     }
                 }
-                vol[(static_cast<size_t>(z) * ny + y) * nx + x] = acc;
+                vol[(static_cast<size_t>(zz) * ny + y) * nx + x] = acc;
             }
         }
     }

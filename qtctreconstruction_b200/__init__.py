@@ -1,0 +1,392 @@
+"""qtctreconstruction_b200 — B200-native backend for QtCTReconstruction's FBP path.
+
+The compute path is ``libctb200.so`` (hand-written sm_100a CUDA kernels behind
+the C ABI declared in ``include/ctb200.h``). This module loads it with ctypes
+and mirrors the reference's ``ct::IReconstructionBackend`` interface
+(IReconstructionBackend.h:10-55) with the same method names, argument meaning
+and result units, so code written against the reference's backends reads the
+same here. There is no CPU fallback: if the library or an sm_100 GPU is
+missing, construction raises.
+
+Conventions (the reference's SerialBackend): slices are ``[y][x]`` float32,
+volumes ``[z][y][x]``, sinograms ``[angle][bin]``; uniform angles are
+``180/na * a`` degrees in float; filter ids follow
+``ReconstructionParams::FilterType``.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+from dataclasses import dataclass, field
+from typing import Callable, Optional
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libctb200.so")
+
+
+class FilterType(enum.IntEnum):
+    """ReconstructionParams::FilterType (CTTypes.h:151)."""
+    Ramp = 0
+    SheppLogan = 1
+    Hamming = 2
+    Cosine = 3
+    Hann = 4
+    Bartlett = 5
+
+
+class Denorm(enum.IntEnum):
+    """Output units of a reconstruction from sinograms (ctb_denorm)."""
+    NONE = 0     # normalised units (SerialBackend::reconstructSlice)
+    SERIAL = 1   # x * (span <= 0 ? 1 : span) + min  (SerialBackend.cpp:297-304)
+    OPENMP = 2   # x * span + min, min if span <= 0  (OpenMPBackend.cpp:37-59)
+
+
+@dataclass
+class ReconstructionParams:
+    """ReconstructionParams (CTTypes.h:150-156)."""
+    filter: FilterType = FilterType.SheppLogan
+    num_angles: int = 180
+    zero_padding: bool = True  # never read by the reference either
+
+
+@dataclass
+class Sinogram:
+    """Sinogram (CTTypes.h:131-137): data is [angle][bin] (height=angles, width=bins)."""
+    data: np.ndarray
+    angles_deg: np.ndarray
+    detector_spacing_mm: float = 1.0
+    original_min_hu: float = 0.0
+    original_max_hu: float = 0.0
+
+
+class CtbError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"ctb status {status}: {message}")
+        self.status = status
+
+
+_lib = None
+_F32P = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+
+
+def library() -> ctypes.CDLL:
+    """Load libctb200.so (raises if it was never built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m qtctreconstruction_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def _declare(L):
+    i, f, p, u64 = ctypes.c_int, ctypes.c_float, ctypes.c_void_p, ctypes.c_uint64
+    P = ctypes.POINTER
+    L.ctb_create.argtypes = [P(p), i]
+    L.ctb_destroy.argtypes = [p]
+    L.ctb_destroy.restype = None
+    L.ctb_last_error.argtypes = [p]
+    L.ctb_last_error.restype = ctypes.c_char_p
+    L.ctb_status_string.argtypes = [i]
+    L.ctb_status_string.restype = ctypes.c_char_p
+    L.ctb_set_stream.argtypes = [p, p]
+    L.ctb_synchronize.argtypes = [p]
+    L.ctb_last_sinogram_ms.argtypes = [p]
+    L.ctb_last_sinogram_ms.restype = ctypes.c_double
+    L.ctb_last_reconstruction_ms.argtypes = [p]
+    L.ctb_last_reconstruction_ms.restype = ctypes.c_double
+    L.ctb_launch_count.argtypes = [p]
+    L.ctb_launch_count.restype = u64
+    L.ctb_pad_geometry.argtypes = [i, P(i), P(i), P(i)]
+    L.ctb_filter_response.argtypes = [i, i, _F32P]
+    L.ctb_compute_sinogram.argtypes = [p, p, i, i, i, i, p, p, p]
+    L.ctb_reconstruct_slice.argtypes = [p, p, i, i, p, i, i, p]
+    L.ctb_reconstruct_volume.argtypes = [p, p, i, i, i, i, i, p]
+    L.ctb_reconstruct_from_sinograms.argtypes = [p, p, i, i, i, p, i, i, p]
+    L.ctb_forward_d.argtypes = [p, p, i, i, i, i, p, p, p]
+    L.ctb_fbp_d.argtypes = [p, p, i, i, i, p, i, i, p, i, p]
+    L.ctb_reconstruct_volume_d.argtypes = [p, p, i, i, i, i, i, p]
+    L.ctb_phantom_params.argtypes = [u64, i, _F32P]
+    L.ctb_phantom_sum_d.argtypes = [p, _F32P, i, i, i, i, p]
+    L.ctb_phantom_sum.argtypes = [p, _F32P, i, i, i, i, p]
+    L.ctb_generator3d.argtypes = [p, i, i, i, f, i, ctypes.c_uint32, _F32P, p]
+    L.ctb_extract_point_cloud.argtypes = [p, p, i, i, i, f, p, ctypes.c_int64, P(ctypes.c_int64)]
+    L.ctb_set_profiling.argtypes = [p, i]
+    L.ctb_stage_times.argtypes = [p, i, P(ctypes.c_double)]
+    L.ctb_probe_smem_bandwidth.argtypes = [p, P(ctypes.c_double)]
+
+
+# ----------------------------------------------------------------- helpers
+def pad_geometry(bins: int):
+    """(square_bins, pad_before, fft_size) of reconstructSlice (SerialBackend.cpp:152-163)."""
+    sq, pad, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    st = library().ctb_pad_geometry(bins, ctypes.byref(sq), ctypes.byref(pad), ctypes.byref(n))
+    if st:
+        raise CtbError(st, "pad_geometry")
+    return sq.value, pad.value, n.value
+
+
+def filter_response(fft_size: int, kind: int) -> np.ndarray:
+    """FilterDesign::createFilter evaluated in double precision (fft_size/2+1 floats)."""
+    H = np.zeros(fft_size // 2 + 1, np.float32)
+    st = library().ctb_filter_response(fft_size, int(kind), H)
+    if st:
+        raise CtbError(st, "filter_response")
+    return H
+
+
+def uniform_angles_deg(na: int) -> np.ndarray:
+    step = np.float32(180.0) / np.float32(na)
+    return (step * np.arange(na, dtype=np.float32)).astype(np.float32)
+
+
+def odd_detector_count(n: int) -> int:
+    """ceil(sqrt(2) * n) rounded up to an odd number (the benchmark detector)."""
+    import math
+    nd = math.ceil(math.sqrt(2.0) * n)
+    return nd + 1 if nd % 2 == 0 else nd
+
+
+def phantom_params(seed: int, count: int) -> np.ndarray:
+    """Benchmark phantom ellipsoids: (count, 16) float32 records."""
+    p = np.zeros(max(count, 1) * 16, np.float32)
+    st = library().ctb_phantom_params(seed, count, p)
+    if st:
+        raise CtbError(st, "phantom_params")
+    return p[: count * 16].reshape(count, 16)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ----------------------------------------------------------------- backend
+class B200Backend:
+    """ct::IReconstructionBackend on one B200 (the new backend type)."""
+
+    def __init__(self, device: int = 0):
+        L = library()
+        h = ctypes.c_void_p()
+        st = L.ctb_create(ctypes.byref(h), device)
+        if st:
+            raise CtbError(st, L.ctb_status_string(st).decode())
+        self._lib = L
+        self._h = h
+        self.device = device
+
+    # -- lifecycle -------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ctb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int, what: str):
+        if st:
+            msg = self._lib.ctb_last_error(self._h).decode()
+            raise CtbError(st, f"{what}: {msg or self._lib.ctb_status_string(st).decode()}")
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- IReconstructionBackend ------------------------------------------
+    def name(self) -> str:
+        return "B200 (CUDA sm_100a)"
+
+    def isAvailable(self) -> bool:
+        return self._h is not None
+
+    def computeSinogram(self, slice2d, num_angles: int, detector_bins: int,
+                        use_parallel: bool = True) -> Sinogram:
+        """SerialBackend::computeSinogram (SerialBackend.cpp:59-136)."""
+        s = _f32(slice2d)
+        if s.ndim != 2 or s.size == 0 or num_angles <= 0 or detector_bins <= 0:
+            return Sinogram(np.zeros((0, 0), np.float32), np.zeros(0, np.float32))
+        h, w = s.shape
+        sino = np.zeros((num_angles, detector_bins), np.float32)
+        ang = np.zeros(num_angles, np.float32)
+        mm = np.zeros(2, np.float32)
+        self._check(self._lib.ctb_compute_sinogram(self._h, _ptr(s), w, h, num_angles, detector_bins,
+                                                   _ptr(sino), _ptr(ang), _ptr(mm)), "computeSinogram")
+        return Sinogram(sino, ang, 1.0, float(mm[0]), float(mm[1]))
+
+    def reconstructSlice(self, sinogram: Sinogram, output_size: int,
+                         params: ReconstructionParams) -> np.ndarray:
+        """SerialBackend::reconstructSlice (SerialBackend.cpp:142-255): normalised units."""
+        d = _f32(sinogram.data)
+        if d.ndim != 2 or d.size == 0 or output_size <= 0:
+            return np.zeros((0, 0), np.float32)
+        na, nd = d.shape
+        ang = _f32(sinogram.angles_deg)
+        out = np.zeros((output_size, output_size), np.float32)
+        self._check(self._lib.ctb_reconstruct_slice(self._h, _ptr(d), na, nd, _ptr(ang), output_size,
+                                                    int(params.filter), _ptr(out)), "reconstructSlice")
+        return out
+
+    def reconstructVolume(self, volume, params: ReconstructionParams,
+                          onSliceDone: Optional[Callable[[int, np.ndarray], None]] = None,
+                          detector_bins: Optional[int] = None) -> np.ndarray:
+        """SerialBackend::reconstructVolume (SerialBackend.cpp:261-318).
+
+        The reference projects onto detector_bins = width; pass detector_bins
+        to use another detector (the benchmark uses odd ceil(sqrt(2) n)).
+        """
+        v = _f32(volume)
+        if v.size == 0:
+            return np.zeros((0, 0, 0), np.float32)
+        nz, n, n2 = v.shape
+        if n != n2:
+            raise ValueError("reconstructVolume needs square slices")
+        nd = n if detector_bins is None else int(detector_bins)
+        out = np.zeros_like(v)
+        self._check(self._lib.ctb_reconstruct_volume(self._h, _ptr(v), n, nz, int(params.num_angles), nd,
+                                                     int(params.filter), _ptr(out)), "reconstructVolume")
+        if onSliceDone:
+            for z in range(nz):
+                onSliceDone(z, out[z])
+        return out
+
+    def reconstructVolumeFromSinograms(self, sinograms, angles_deg, params: ReconstructionParams,
+                                       onSliceDone: Optional[Callable[[int, np.ndarray], None]] = None,
+                                       denorm: Denorm = Denorm.NONE) -> np.ndarray:
+        """IReconstructionBackend::reconstructVolumeFromSinograms (IReconstructionBackend.h:39-44).
+
+        The default (Denorm.NONE) stores reconstructSlice's normalised units,
+        as the interface's default per-slice loop does with SerialBackend.
+        """
+        s = _f32(sinograms)
+        if s.size == 0:
+            return np.zeros((0, 0, 0), np.float32)
+        nz, na, bins = s.shape
+        ang = _f32(angles_deg)
+        out = np.zeros((nz, bins, bins), np.float32)
+        self._check(self._lib.ctb_reconstruct_from_sinograms(self._h, _ptr(s), nz, na, bins, _ptr(ang),
+                                                             int(params.filter), int(denorm), _ptr(out)),
+                    "reconstructVolumeFromSinograms")
+        if onSliceDone:
+            for z in range(nz):
+                onSliceDone(z, out[z])
+        return out
+
+    def extractPointCloud(self, vol, threshold: float) -> np.ndarray:
+        """Points (x, y, z, hu) with hu > threshold, index coordinates, z/y/x order."""
+        v = _f32(vol)
+        if v.size == 0:
+            return np.zeros((0, 4), np.float32)
+        nz, ny, nx = v.shape
+        cnt = ctypes.c_int64()
+        self._check(self._lib.ctb_extract_point_cloud(self._h, _ptr(v), nx, ny, nz, float(threshold), None, 0,
+                                                      ctypes.byref(cnt)), "extractPointCloud")
+        pts = np.zeros((cnt.value, 4), np.float32)
+        if cnt.value:
+            self._check(self._lib.ctb_extract_point_cloud(self._h, _ptr(v), nx, ny, nz, float(threshold),
+                                                          _ptr(pts), cnt.value, ctypes.byref(cnt)),
+                        "extractPointCloud")
+        return pts
+
+    def lastSinogramTimeMs(self) -> float:
+        return float(self._lib.ctb_last_sinogram_ms(self._h))
+
+    def lastReconstructionTimeMs(self) -> float:
+        return float(self._lib.ctb_last_reconstruction_ms(self._h))
+
+    # -- phantoms ----------------------------------------------------------
+    def phantom(self, params: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
+        p = _f32(params).reshape(-1)
+        vol = np.zeros((nz, ny, nx), np.float32)
+        self._check(self._lib.ctb_phantom_sum(self._h, p, p.size // 16, nx, ny, nz, _ptr(vol)), "phantom")
+        return vol
+
+    def generator3d(self, nx: int, ny: int, nz: int, radius_mm=50.0, count=120, seed=42,
+                    tissue=None) -> np.ndarray:
+        """Generator3D::generateBrainHU (Generator3DCPU.cpp:94-117) on the GPU."""
+        t = _f32(tissue if tissue is not None else GENERATOR3D_TISSUE)
+        vol = np.zeros((nz, ny, nx), np.float32)
+        self._check(self._lib.ctb_generator3d(self._h, nx, ny, nz, float(radius_mm), int(count), int(seed), t,
+                                              _ptr(vol)), "generator3d")
+        return vol
+
+    # -- device-resident entry points (torch tensors or raw pointers) -------
+    def set_stream(self, stream_handle: int):
+        self._check(self._lib.ctb_set_stream(self._h, ctypes.c_void_p(stream_handle)), "set_stream")
+
+    def synchronize(self):
+        self._check(self._lib.ctb_synchronize(self._h), "synchronize")
+
+    def launch_count(self) -> int:
+        return int(self._lib.ctb_launch_count(self._h))
+
+    def forward_d(self, d_vol: int, n: int, depth: int, na: int, nd: int, d_sino: int, d_stats: int,
+                  angles_deg=None):
+        ang = None if angles_deg is None else _f32(angles_deg)
+        self._check(self._lib.ctb_forward_d(self._h, ctypes.c_void_p(d_vol), n, depth, na, nd,
+                                            None if ang is None else _ptr(ang), ctypes.c_void_p(d_sino),
+                                            ctypes.c_void_p(d_stats)), "forward_d")
+
+    def fbp_d(self, d_sino: int, depth: int, na: int, bins: int, output_size: int, kind: int,
+              d_out: int, d_stats: int = 0, denorm: Denorm = Denorm.NONE, angles_deg=None):
+        ang = None if angles_deg is None else _f32(angles_deg)
+        self._check(self._lib.ctb_fbp_d(self._h, ctypes.c_void_p(d_sino), depth, na, bins,
+                                        None if ang is None else _ptr(ang), output_size, int(kind),
+                                        ctypes.c_void_p(d_stats) if d_stats else None, int(denorm),
+                                        ctypes.c_void_p(d_out)), "fbp_d")
+
+    def reconstruct_volume_host(self, host_vol: int, n: int, depth: int, na: int, nd: int, kind: int,
+                                host_out: int):
+        """reconstructVolume through the host-buffer C ABI call on raw (e.g. pinned) pointers."""
+        self._check(self._lib.ctb_reconstruct_volume(self._h, ctypes.c_void_p(host_vol), n, depth, na, nd,
+                                                     int(kind), ctypes.c_void_p(host_out)), "reconstructVolume")
+
+    def set_profiling(self, enable: bool = True):
+        self._check(self._lib.ctb_set_profiling(self._h, int(bool(enable))), "set_profiling")
+
+    def stage_times(self, back: int = 0):
+        """Device ms of {stats+normalise, forward, filter, backprojection} of a profiled call."""
+        t = (ctypes.c_double * 4)()
+        self._check(self._lib.ctb_stage_times(self._h, back, t), "stage_times")
+        return list(t)
+
+    def probe_smem_bandwidth(self) -> float:
+        g = ctypes.c_double()
+        self._check(self._lib.ctb_probe_smem_bandwidth(self._h, ctypes.byref(g)), "probe_smem_bandwidth")
+        return g.value
+
+    def reconstruct_volume_d(self, d_vol: int, n: int, depth: int, na: int, nd: int, kind: int, d_out: int):
+        self._check(self._lib.ctb_reconstruct_volume_d(self._h, ctypes.c_void_p(d_vol), n, depth, na, nd,
+                                                       int(kind), ctypes.c_void_p(d_out)), "reconstruct_volume_d")
+
+    def phantom_d(self, params: np.ndarray, nx: int, ny: int, nz: int, d_vol: int):
+        p = _f32(params).reshape(-1)
+        self._check(self._lib.ctb_phantom_sum_d(self._h, p, p.size // 16, nx, ny, nz, ctypes.c_void_p(d_vol)),
+                    "phantom_d")
+
+
+# Generator3D::Params defaults (Generator3D.h:16-34): soft tissue, then bone.
+GENERATOR3D_TISSUE = np.array(
+    [-20.0, 45.0, 3.0, 10.0, 0.0, 0.0, 0.0, 1.0,
+     200.0, 1000.0, 2.0, 8.0, 1.0, 0.7, 0.9, 0.15], dtype=np.float32)
+
+__all__ = ["B200Backend", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
+           "library", "pad_geometry", "filter_response", "uniform_angles_deg", "odd_detector_count",
+           "phantom_params", "GENERATOR3D_TISSUE", "LIB_PATH"]

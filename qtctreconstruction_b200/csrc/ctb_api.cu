@@ -1,0 +1,655 @@
+// ctb_api.cu — the extern "C" entry points of libctb200.so (include/ctb200.h)
+// and the orchestration of the forward / filter / backprojection stages.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "ctb_internal.h"
+
+namespace ctb {
+cudaError_t launch_phantom_sum_boxes(const float* d_params, const int* d_boxes, int k, int nx,
+                                     int ny, int nz, float* d_vol, cudaStream_t st);
+cudaError_t launch_generator3d_boxes(const float* d_ell, const int* d_boxes, int k, int nx,
+                                     int ny, int nz, float radius_mm, float* d_vol,
+                                     cudaStream_t st);
+void phantom_params(uint64_t seed, int count, float* out);
+void phantom_boxes(const float* params, int count, int nx, int ny, int nz, int* boxes);
+void generator3d_params(float radius, int count, uint32_t seed, const float* tissue, float* ell);
+void generator3d_boxes(const float* ell, int count, int nx, int ny, int nz, float radius,
+                       int* boxes);
+cudaError_t smem_probe(int sms, float* d_out, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1,
+                       double* bytes);
+
+void* workspace(ctb_ctx* ctx, const std::string& name, size_t bytes) {
+    DevBuf& b = ctx->ws[name];
+    if (b.bytes >= bytes && b.ptr) return b.ptr;
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+    const size_t want = std::max<size_t>(bytes, 256);
+    if (cudaMalloc(&b.ptr, want) != cudaSuccess) {
+        cudaGetLastError();
+        b.ptr = nullptr;
+        return nullptr;
+    }
+    b.bytes = want;
+    return b.ptr;
+}
+}  // namespace ctb
+
+using namespace ctb;
+
+namespace {
+
+constexpr int kMaxAngles = 1 << 16;
+constexpr int kMaxFft = 8192;
+
+ctb_status fail(ctb_ctx* ctx, ctb_status s, const char* fmt, ...) {
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        ctx->last_error = buf;
+    }
+    return s;
+}
+
+#define CTB_CUDA(ctx, call)                                                                    \
+    do {                                                                                       \
+        const cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail((ctx), e_ == cudaErrorMemoryAllocation ? CTB_ERR_OOM : CTB_ERR_CUDA,   \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+#define CTB_LAUNCH(ctx, call)       \
+    do {                            \
+        CTB_CUDA(ctx, (call));      \
+        ++(ctx)->launches;          \
+    } while (0)
+
+#define CTB_TRY(expr)                 \
+    do {                              \
+        const ctb_status s_ = (expr); \
+        if (s_ != CTB_OK) return s_;  \
+    } while (0)
+
+template <typename T>
+T* ws(ctb_ctx* ctx, const char* name, size_t count) {
+    return static_cast<T*>(workspace(ctx, name, count * sizeof(T)));
+}
+
+#define CTB_WS(ctx, var, T, name, count)                                                  \
+    T* var = ws<T>((ctx), (name), (count));                                               \
+    if (!var) return fail((ctx), CTB_ERR_OOM, "device workspace '%s' (%zu bytes) failed", \
+                          (name), static_cast<size_t>(count) * sizeof(T))
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Float degrees 180/na * a (SerialBackend.cpp:126-130).
+std::vector<float> uniform_angles(int na) {
+    std::vector<float> a(na);
+    const float step = 180.0f / static_cast<float>(na);
+    for (int i = 0; i < na; ++i) a[i] = step * static_cast<float>(i);
+    return a;
+}
+
+// cos/sin table (double) of the angles on the device. Uniform angles
+// (angles_deg == NULL, 180/na * a in float) are cached per count; an explicit
+// angle list is re-uploaded only when it differs from the previous one.
+ctb_status trig_table(ctb_ctx* ctx, const float* angles_deg, int na, const double2** out) {
+    if (!angles_deg) {
+        auto it = ctx->trig_uniform.find(na);
+        if (it == ctx->trig_uniform.end()) {
+            const std::vector<float> uni = uniform_angles(na);
+            DevBuf deg, cs;
+            CTB_CUDA(ctx, cudaMalloc(&deg.ptr, sizeof(float) * na));
+            CTB_CUDA(ctx, cudaMalloc(&cs.ptr, sizeof(double2) * na));
+            CTB_CUDA(ctx, cudaMemcpy(deg.ptr, uni.data(), sizeof(float) * na, cudaMemcpyHostToDevice));
+            CTB_LAUNCH(ctx, launch_trig(static_cast<float*>(deg.ptr), na, static_cast<double2*>(cs.ptr),
+                                        ctx->stream));
+            CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            cudaFree(deg.ptr);
+            cs.bytes = sizeof(double2) * na;
+            it = ctx->trig_uniform.emplace(na, cs).first;
+        }
+        *out = static_cast<const double2*>(it->second.ptr);
+        return CTB_OK;
+    }
+    CTB_WS(ctx, d_cs, double2, "trig_user", na);
+    if (ctx->user_angles.size() != static_cast<size_t>(na) ||
+        std::memcmp(ctx->user_angles.data(), angles_deg, sizeof(float) * na) != 0) {
+        CTB_WS(ctx, d_deg, float, "angles_user", na);
+        CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // previous users of the table are done
+        CTB_CUDA(ctx, cudaMemcpy(d_deg, angles_deg, sizeof(float) * na, cudaMemcpyHostToDevice));
+        CTB_LAUNCH(ctx, launch_trig(d_deg, na, d_cs, ctx->stream));
+        ctx->user_angles.assign(angles_deg, angles_deg + na);
+    }
+    *out = d_cs;
+    return CTB_OK;
+}
+
+// Filter spectrum for the complex-pair FFT: Hs[k] = H[min(k, L-k)] / L with
+// Hs[0] = Hs[L/2] = 0 (the reference's inverse transform drops the Nyquist bin).
+ctb_status filter_tables(ctb_ctx* ctx, int L, int type, const float** d_Hs, const float2** d_tw) {
+    auto key = std::make_pair(L, type);
+    auto it = ctx->filters.find(key);
+    if (it == ctx->filters.end()) {
+        const std::vector<double> H = filter_response(L, type);
+        std::vector<float> Hs(L);
+        for (int k = 0; k < L; ++k) {
+            const int m = k <= L / 2 ? k : L - k;
+            Hs[k] = static_cast<float>(H[m] / L);
+        }
+        Hs[0] = 0.0f;
+        Hs[L / 2] = 0.0f;
+        DevBuf b;
+        CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float) * L));
+        b.bytes = sizeof(float) * L;
+        CTB_CUDA(ctx, cudaMemcpy(b.ptr, Hs.data(), b.bytes, cudaMemcpyHostToDevice));
+        it = ctx->filters.emplace(key, b).first;
+    }
+    auto jt = ctx->twiddles.find(L);
+    if (jt == ctx->twiddles.end()) {
+        std::vector<float2> tw(L);
+        for (int i = 0; i < L; ++i) {
+            const double ang = 2.0 * 3.14159265358979323846 * static_cast<double>(i) / L;
+            tw[i] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(-std::sin(ang)));
+        }
+        DevBuf b;
+        CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float2) * L));
+        b.bytes = sizeof(float2) * L;
+        CTB_CUDA(ctx, cudaMemcpy(b.ptr, tw.data(), b.bytes, cudaMemcpyHostToDevice));
+        jt = ctx->twiddles.emplace(L, b).first;
+    }
+    *d_Hs = static_cast<const float*>(it->second.ptr);
+    *d_tw = static_cast<const float2*>(jt->second.ptr);
+    return CTB_OK;
+}
+
+struct Guard {
+    ctb_ctx* ctx;
+    std::lock_guard<std::recursive_mutex> lock;
+    explicit Guard(ctb_ctx* c) : ctx(c), lock(c->mu) { cudaSetDevice(c->device); }
+};
+
+ctb_status check_error_word(ctb_ctx* ctx) {
+    unsigned h = 0;
+    CTB_CUDA(ctx, cudaMemcpyAsync(&h, ctx->d_err, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h) {
+        cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), ctx->stream);
+        return fail(ctx, CTB_ERR_TIMEOUT, "a bounded device wait gave up (code %u)", h);
+    }
+    return CTB_OK;
+}
+
+// ------------------------------------------------------------ stages
+// Record profiling event `k` of the current set (no-op when `ev` is null).
+void mark(ctb_ctx* ctx, cudaEvent_t* ev, int k) {
+    if (ev) cudaEventRecord(ev[k], ctx->stream);
+}
+
+ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz, int na, int nd,
+                         const float* angles_deg, float* d_sino, float4* d_stats,
+                         cudaEvent_t* ev = nullptr) {
+    const int nzg = (nz + 3) / 4;
+    const size_t img = static_cast<size_t>(nzg) * w * h;
+    CTB_WS(ctx, d_img, float4, "img", img);
+    CTB_WS(ctx, d_imgT, float4, "imgT", img);
+    const double2* d_cs = nullptr;
+    CTB_TRY(trig_table(ctx, angles_deg, na, &d_cs));
+    CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream));
+    CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream));
+    mark(ctx, ev, 1);
+    CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd, d_cs, d_sino, ctx->stream));
+    return CTB_OK;
+}
+
+ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins,
+                     const float* angles_deg, int n_out, int filter, const float4* d_stats,
+                     int denorm, float* d_out, cudaEvent_t* ev = nullptr) {
+    const PadGeom g = pad_geometry(bins);
+    if (g.L > kMaxFft)
+        return fail(ctx, CTB_ERR_UNSUPPORTED, "fft size %d (bins %d) exceeds %d", g.L, bins, kMaxFft);
+    const FiltLayout fl = filt_layout(g.sq, n_out);
+    const int nzg = (nz + 3) / 4;
+    CTB_WS(ctx, d_filt, float4, "filt", static_cast<size_t>(nzg) * na * fl.pitch);
+    const float* d_Hs = nullptr;
+    const float2* d_tw = nullptr;
+    CTB_TRY(filter_tables(ctx, g.L, filter, &d_Hs, &d_tw));
+    const double2* d_cs = nullptr;
+    CTB_TRY(trig_table(ctx, angles_deg, na, &d_cs));
+    // SerialBackend.cpp:246: pi / (2 na) in float
+    const float scale = 3.14159265358979323846f / (2.0f * static_cast<float>(na));
+    CTB_LAUNCH(ctx, launch_filter(d_sino, nz, na, g, fl, d_Hs, d_tw, d_stats, denorm, scale, d_filt,
+                                  ctx->stream));
+    mark(ctx, ev, 3);
+    CTB_LAUNCH(ctx, launch_backproject(d_filt, nz, na, fl, n_out, d_cs, d_stats, denorm, d_out,
+                                       ctx->d_err, ctx->stream));
+    return CTB_OK;
+}
+
+ctb_status check_common(ctb_ctx* ctx) {
+    if (!ctx) return CTB_ERR_INVALID;
+    return CTB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ctb_status_string(ctb_status s) {
+    switch (s) {
+    case CTB_OK: return "ok";
+    case CTB_ERR_INVALID: return "invalid argument";
+    case CTB_ERR_CUDA: return "CUDA error";
+    case CTB_ERR_OOM: return "out of device memory";
+    case CTB_ERR_UNSUPPORTED: return "unsupported size";
+    case CTB_ERR_NO_DEVICE: return "no sm_100 device";
+    case CTB_ERR_TIMEOUT: return "device wait timed out";
+    case CTB_ERR_CANCELLED: return "cancelled";
+    case CTB_ERR_NOT_FOUND: return "not found";
+    case CTB_ERR_BUSY: return "busy";
+    }
+    return "unknown status";
+}
+
+ctb_status ctb_create(ctb_ctx** out, int device) {
+    if (!out) return CTB_ERR_INVALID;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return CTB_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+        cudaGetLastError();
+        return CTB_ERR_NO_DEVICE;
+    }
+    auto* ctx = new ctb_ctx();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&ctx->d_err, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(ctx->d_err, 0, sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return CTB_ERR_CUDA;
+    }
+    for (auto& e : ctx->ev) cudaEventCreate(&e);
+    ctx->stream = ctx->own_stream;
+    *out = ctx;
+    return CTB_OK;
+}
+
+void ctb_destroy(ctb_ctx* ctx) {
+    if (!ctx) return;
+    {
+        std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        for (auto& kv : ctx->ws) cudaFree(kv.second.ptr);
+        for (auto& kv : ctx->filters) cudaFree(kv.second.ptr);
+        for (auto& kv : ctx->twiddles) cudaFree(kv.second.ptr);
+        for (auto& kv : ctx->trig_uniform) cudaFree(kv.second.ptr);
+        for (auto& e : ctx->prof_ev)
+            if (e) cudaEventDestroy(e);
+        for (auto& e : ctx->ev)
+            if (e) cudaEventDestroy(e);
+        if (ctx->d_err) cudaFree(ctx->d_err);
+        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    }
+    delete ctx;
+}
+
+const char* ctb_last_error(const ctb_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+ctb_status ctb_set_stream(ctb_ctx* ctx, void* stream) {
+    if (!ctx) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return CTB_OK;
+}
+
+ctb_status ctb_synchronize(ctb_ctx* ctx) {
+    if (!ctx) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return check_error_word(ctx);
+}
+
+double ctb_last_sinogram_ms(const ctb_ctx* ctx) { return ctx ? ctx->last_sino_ms : 0.0; }
+double ctb_last_reconstruction_ms(const ctb_ctx* ctx) { return ctx ? ctx->last_recon_ms : 0.0; }
+uint64_t ctb_launch_count(const ctb_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+ctb_status ctb_pad_geometry(int bins, int* square_bins, int* pad_before, int* fft_size) {
+    if (bins <= 0 || !square_bins || !pad_before || !fft_size) return CTB_ERR_INVALID;
+    const PadGeom g = pad_geometry(bins);
+    *square_bins = g.sq;
+    *pad_before = g.pad;
+    *fft_size = g.L;
+    return CTB_OK;
+}
+
+ctb_status ctb_filter_response(int fft_size, int filter, float* H) {
+    if (fft_size < 2 || (fft_size & (fft_size - 1)) || !H) return CTB_ERR_INVALID;
+    const auto v = filter_response(fft_size, filter);
+    for (size_t i = 0; i < v.size(); ++i) H[i] = static_cast<float>(v[i]);
+    return CTB_OK;
+}
+
+ctb_status ctb_set_profiling(ctb_ctx* ctx, int enable) {
+    if (!ctx) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    if (enable && ctx->prof_ev.empty()) {
+        ctx->prof_ev.resize(ctb_ctx::kProfRing * ctb_ctx::kProfEvents);
+        for (auto& e : ctx->prof_ev) CTB_CUDA(ctx, cudaEventCreate(&e));
+    }
+    ctx->profiling = enable != 0;
+    return CTB_OK;
+}
+
+ctb_status ctb_stage_times(ctb_ctx* ctx, int back, double* ms) {
+    if (!ctx || !ms || back < 0 || back >= ctb_ctx::kProfRing || back >= ctx->prof_calls ||
+        ctx->prof_ev.empty())
+        return fail(ctx, CTB_ERR_INVALID, "ctb_stage_times: no such profiled call");
+    Guard g(ctx);
+    const long long idx = (ctx->prof_calls - 1 - back) % ctb_ctx::kProfRing;
+    cudaEvent_t* ev = &ctx->prof_ev[idx * ctb_ctx::kProfEvents];
+    CTB_CUDA(ctx, cudaEventSynchronize(ev[ctb_ctx::kProfEvents - 1]));
+    for (int k = 0; k + 1 < ctb_ctx::kProfEvents; ++k) {
+        float t = 0.f;
+        CTB_CUDA(ctx, cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+        ms[k] = t;
+    }
+    return CTB_OK;
+}
+
+ctb_status ctb_probe_smem_bandwidth(ctb_ctx* ctx, double* gbs) {
+    if (!ctx || !gbs) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    int sms = 0;
+    CTB_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    CTB_WS(ctx, d_out, float, "probe_out", 4 * sms);
+    double bytes = 0.0;
+    CTB_LAUNCH(ctx, smem_probe(sms, d_out, ctx->stream, ctx->ev[0], ctx->ev[1], &bytes));
+    ++ctx->launches;  // warm-up launch
+    CTB_CUDA(ctx, cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0.f;
+    CTB_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    *gbs = bytes / (ms * 1e-3) / 1e9;
+    return CTB_OK;
+}
+
+// ------------------------------------------------- device-buffer entry points
+ctb_status ctb_forward_d(ctb_ctx* ctx, const float* d_vol, int n, int depth, int num_angles,
+                         int detector_bins, const float* angles_deg, float* d_sino,
+                         float* d_stats) {
+    CTB_TRY(check_common(ctx));
+    if (!d_vol || !d_sino || !d_stats || n <= 0 || depth <= 0 || num_angles <= 0 ||
+        detector_bins <= 0 || num_angles > kMaxAngles)
+        return fail(ctx, CTB_ERR_INVALID, "ctb_forward_d: invalid arguments");
+    if (!aligned16(d_stats)) return fail(ctx, CTB_ERR_INVALID, "d_stats must be 16-byte aligned");
+    Guard g(ctx);
+    return forward_stage(ctx, d_vol, n, n, depth, num_angles, detector_bins, angles_deg, d_sino,
+                         reinterpret_cast<float4*>(d_stats));
+}
+
+ctb_status ctb_fbp_d(ctb_ctx* ctx, const float* d_sino, int depth, int num_angles, int bins,
+                     const float* angles_deg, int output_size, int filter, const float* d_stats,
+                     int denorm, float* d_out) {
+    CTB_TRY(check_common(ctx));
+    if (!d_sino || !d_out || depth <= 0 || num_angles <= 0 || bins <= 0 || output_size <= 0 ||
+        num_angles > kMaxAngles || denorm < 0 || denorm > 2)
+        return fail(ctx, CTB_ERR_INVALID, "ctb_fbp_d: invalid arguments");
+    if (d_stats && !aligned16(d_stats)) return fail(ctx, CTB_ERR_INVALID, "d_stats must be 16-byte aligned");
+    Guard g(ctx);
+    return fbp_stage(ctx, d_sino, depth, num_angles, bins, angles_deg, output_size, filter,
+                     reinterpret_cast<const float4*>(d_stats), d_stats ? denorm : CTB_DENORM_NONE,
+                     d_out);
+}
+
+ctb_status ctb_reconstruct_volume_d(ctb_ctx* ctx, const float* d_vol, int n, int depth,
+                                    int num_angles, int detector_bins, int filter, float* d_out) {
+    CTB_TRY(check_common(ctx));
+    if (!d_vol || !d_out || n <= 0 || depth <= 0 || num_angles <= 0 || detector_bins <= 0 ||
+        num_angles > kMaxAngles)
+        return fail(ctx, CTB_ERR_INVALID, "ctb_reconstruct_volume_d: invalid arguments");
+    Guard g(ctx);
+    CTB_WS(ctx, d_sino, float, "sino", static_cast<size_t>(depth) * num_angles * detector_bins);
+    CTB_WS(ctx, d_stats, float4, "stats", depth);
+    cudaEvent_t* pev = nullptr;
+    if (ctx->profiling) {
+        pev = &ctx->prof_ev[(ctx->prof_calls % ctb_ctx::kProfRing) * ctb_ctx::kProfEvents];
+        ++ctx->prof_calls;
+    }
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+    mark(ctx, pev, 0);
+    CTB_TRY(forward_stage(ctx, d_vol, n, n, depth, num_angles, detector_bins, nullptr, d_sino, d_stats,
+                          pev));
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+    mark(ctx, pev, 2);
+    CTB_TRY(fbp_stage(ctx, d_sino, depth, num_angles, detector_bins, nullptr, n, filter, d_stats,
+                      CTB_DENORM_SERIAL, d_out, pev));
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+    mark(ctx, pev, 4);
+    return CTB_OK;
+}
+
+// --------------------------------------------------- host-buffer entry points
+ctb_status ctb_compute_sinogram(ctb_ctx* ctx, const float* slice, int width, int height,
+                                int num_angles, int detector_bins, float* sino_out,
+                                float* angles_deg_out, float* minmax_out) {
+    CTB_TRY(check_common(ctx));
+    if (!slice || !sino_out || width <= 0 || height <= 0 || num_angles <= 0 ||
+        detector_bins <= 0 || num_angles > kMaxAngles)
+        return fail(ctx, CTB_ERR_INVALID, "ctb_compute_sinogram: invalid arguments");
+    Guard g(ctx);
+    const size_t npx = static_cast<size_t>(width) * height;
+    const size_t ns = static_cast<size_t>(num_angles) * detector_bins;
+    CTB_WS(ctx, d_in, float, "h_in", npx);
+    CTB_WS(ctx, d_sino, float, "h_sino", ns);
+    CTB_WS(ctx, d_stats, float4, "h_stats", 1);
+    CTB_CUDA(ctx, cudaMemcpyAsync(d_in, slice, npx * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+    CTB_TRY(forward_stage(ctx, d_in, width, height, 1, num_angles, detector_bins, nullptr, d_sino, d_stats));
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+    CTB_CUDA(ctx, cudaMemcpyAsync(sino_out, d_sino, ns * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    float4 st;
+    CTB_CUDA(ctx, cudaMemcpyAsync(&st, d_stats, sizeof st, cudaMemcpyDeviceToHost, ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    ctx->last_sino_ms = ms;
+    if (angles_deg_out) {
+        const auto a = uniform_angles(num_angles);
+        std::memcpy(angles_deg_out, a.data(), sizeof(float) * num_angles);
+    }
+    if (minmax_out) { minmax_out[0] = st.x; minmax_out[1] = st.y; }
+    return check_error_word(ctx);
+}
+
+ctb_status ctb_reconstruct_slice(ctb_ctx* ctx, const float* sino, int num_angles,
+                                 int detector_bins, const float* angles_deg, int output_size,
+                                 int filter, float* out) {
+    CTB_TRY(check_common(ctx));
+    if (!sino || !out || !angles_deg || num_angles <= 0 || detector_bins <= 0 ||
+        output_size <= 0 || num_angles > kMaxAngles)
+        return fail(ctx, CTB_ERR_INVALID, "ctb_reconstruct_slice: invalid arguments");
+    Guard g(ctx);
+    const size_t ns = static_cast<size_t>(num_angles) * detector_bins;
+    const size_t no = static_cast<size_t>(output_size) * output_size;
+    CTB_WS(ctx, d_sino, float, "h_sino", ns);
+    CTB_WS(ctx, d_out, float, "h_out", no);
+    CTB_CUDA(ctx, cudaMemcpyAsync(d_sino, sino, ns * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+    CTB_TRY(fbp_stage(ctx, d_sino, 1, num_angles, detector_bins, angles_deg, output_size, filter,
+                      nullptr, CTB_DENORM_NONE, d_out));
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+    CTB_CUDA(ctx, cudaMemcpyAsync(out, d_out, no * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+    ctx->last_recon_ms = ms;
+    return check_error_word(ctx);
+}
+
+ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int depth,
+                                  int num_angles, int detector_bins, int filter, float* out) {
+    CTB_TRY(check_common(ctx));
+    if (!vol || !out || n <= 0 || depth <= 0 || num_angles <= 0 || detector_bins <= 0)
+        return fail(ctx, CTB_ERR_INVALID, "ctb_reconstruct_volume: invalid arguments");
+    Guard g(ctx);
+    const size_t nv = static_cast<size_t>(depth) * n * n;
+    CTB_WS(ctx, d_in, float, "h_in", nv);
+    CTB_WS(ctx, d_out, float, "h_out", nv);
+    CTB_CUDA(ctx, cudaMemcpyAsync(d_in, vol, nv * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CTB_TRY(ctb_reconstruct_volume_d(ctx, d_in, n, depth, num_angles, detector_bins, filter, d_out));
+    CTB_CUDA(ctx, cudaMemcpyAsync(out, d_out, nv * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+    ctx->last_sino_ms = a;
+    ctx->last_recon_ms = b;
+    return check_error_word(ctx);
+}
+
+ctb_status ctb_reconstruct_from_sinograms(ctb_ctx* ctx, const float* sinos, int depth,
+                                          int num_angles, int bins, const float* angles_deg,
+                                          int filter, int denorm, float* out) {
+    CTB_TRY(check_common(ctx));
+    if (!sinos || !out || !angles_deg || depth <= 0 || num_angles <= 0 || bins <= 0 ||
+        denorm < 0 || denorm > 2)
+        return fail(ctx, CTB_ERR_INVALID, "ctb_reconstruct_from_sinograms: invalid arguments");
+    Guard g(ctx);
+    const size_t ns = static_cast<size_t>(depth) * num_angles * bins;
+    const size_t no = static_cast<size_t>(depth) * bins * bins;
+    CTB_WS(ctx, d_sino, float, "h_sino", ns);
+    CTB_WS(ctx, d_out, float, "h_out", no);
+    CTB_WS(ctx, d_stats, float4, "h_stats", depth);
+    CTB_CUDA(ctx, cudaMemcpyAsync(d_sino, sinos, ns * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+    if (denorm != CTB_DENORM_NONE)  // BackendFactory.cpp:41-51: min/max of the sinogram itself
+        CTB_LAUNCH(ctx, launch_slice_stats(d_sino, static_cast<long long>(num_angles) * bins, depth,
+                                           d_stats, ctx->stream));
+    CTB_TRY(fbp_stage(ctx, d_sino, depth, num_angles, bins, angles_deg, bins, filter,
+                      denorm != CTB_DENORM_NONE ? d_stats : nullptr, denorm, d_out));
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+    CTB_CUDA(ctx, cudaMemcpyAsync(out, d_out, no * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+    ctx->last_recon_ms = ms;
+    ctx->last_sino_ms = 0.0;
+    return check_error_word(ctx);
+}
+
+// ------------------------------------------------------------------ phantoms
+ctb_status ctb_phantom_params(uint64_t seed, int count, float* params) {
+    if (count < 0 || (count > 0 && !params)) return CTB_ERR_INVALID;
+    phantom_params(seed, count, params);
+    return CTB_OK;
+}
+
+ctb_status ctb_phantom_sum_d(ctb_ctx* ctx, const float* params, int count, int nx, int ny,
+                             int nz, float* d_vol) {
+    CTB_TRY(check_common(ctx));
+    if (count < 0 || (count > 0 && !params) || !d_vol || nx <= 0 || ny <= 0 || nz <= 0 || count > 32767)
+        return fail(ctx, CTB_ERR_INVALID, "ctb_phantom_sum_d: invalid arguments");
+    Guard g(ctx);
+    std::vector<int> boxes(6 * static_cast<size_t>(std::max(count, 1)));
+    if (count) phantom_boxes(params, count, nx, ny, nz, boxes.data());
+    CTB_WS(ctx, d_p, float, "phantom_params", 16 * static_cast<size_t>(std::max(count, 1)));
+    CTB_WS(ctx, d_b, int, "phantom_boxes", boxes.size());
+    if (count) {
+        CTB_CUDA(ctx, cudaMemcpyAsync(d_p, params, sizeof(float) * 16 * count, cudaMemcpyHostToDevice, ctx->stream));
+        CTB_CUDA(ctx, cudaMemcpyAsync(d_b, boxes.data(), sizeof(int) * 6 * count, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CTB_LAUNCH(ctx, launch_phantom_sum_boxes(d_p, d_b, count, nx, ny, nz, d_vol, ctx->stream));
+    // the host vectors must outlive the asynchronous copies
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return CTB_OK;
+}
+
+ctb_status ctb_phantom_sum(ctb_ctx* ctx, const float* params, int count, int nx, int ny, int nz,
+                           float* vol) {
+    CTB_TRY(check_common(ctx));
+    if (!vol || nx <= 0 || ny <= 0 || nz <= 0) return fail(ctx, CTB_ERR_INVALID, "ctb_phantom_sum: invalid arguments");
+    Guard g(ctx);
+    const size_t nv = static_cast<size_t>(nx) * ny * nz;
+    CTB_WS(ctx, d_vol, float, "h_out", nv);
+    CTB_TRY(ctb_phantom_sum_d(ctx, params, count, nx, ny, nz, d_vol));
+    CTB_CUDA(ctx, cudaMemcpyAsync(vol, d_vol, nv * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return CTB_OK;
+}
+
+ctb_status ctb_generator3d(ctb_ctx* ctx, int nx, int ny, int nz, float radius_mm, int count,
+                           uint32_t seed, const float* tissue, float* vol) {
+    CTB_TRY(check_common(ctx));
+    if (!vol || !tissue || nx <= 0 || ny <= 0 || nz <= 0 || count < 0 || count > 32767)
+        return fail(ctx, CTB_ERR_INVALID, "ctb_generator3d: invalid arguments");
+    Guard g(ctx);
+    const int k = std::max(count, 1);
+    std::vector<float> ell(7 * static_cast<size_t>(k), 0.0f);
+    std::vector<int> boxes(6 * static_cast<size_t>(k), 0);
+    if (count) {
+        generator3d_params(radius_mm, count, seed, tissue, ell.data());
+        generator3d_boxes(ell.data(), count, nx, ny, nz, radius_mm, boxes.data());
+    }
+    const size_t nv = static_cast<size_t>(nx) * ny * nz;
+    CTB_WS(ctx, d_vol, float, "h_out", nv);
+    CTB_WS(ctx, d_e, float, "gen_ell", ell.size());
+    CTB_WS(ctx, d_b, int, "gen_boxes", boxes.size());
+    CTB_CUDA(ctx, cudaMemcpyAsync(d_e, ell.data(), sizeof(float) * ell.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CTB_CUDA(ctx, cudaMemcpyAsync(d_b, boxes.data(), sizeof(int) * boxes.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CTB_LAUNCH(ctx, launch_generator3d_boxes(d_e, d_b, count, nx, ny, nz, radius_mm, d_vol, ctx->stream));
+    CTB_CUDA(ctx, cudaMemcpyAsync(vol, d_vol, nv * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return CTB_OK;
+}
+
+// --------------------------------------------------------------- point cloud
+ctb_status ctb_extract_point_cloud(ctb_ctx* ctx, const float* vol, int nx, int ny, int nz,
+                                   float threshold, float* points, int64_t capacity,
+                                   int64_t* count) {
+    CTB_TRY(check_common(ctx));
+    if (!vol || !count || nx <= 0 || ny <= 0 || nz <= 0 || capacity < 0 || (capacity > 0 && !points))
+        return fail(ctx, CTB_ERR_INVALID, "ctb_extract_point_cloud: invalid arguments");
+    Guard g(ctx);
+    const long long total = static_cast<long long>(nx) * ny * nz;
+    const int blocks = point_blocks(total);
+    CTB_WS(ctx, d_vol, float, "h_in", total);
+    CTB_WS(ctx, d_cnt, unsigned, "pc_counts", blocks);
+    CTB_WS(ctx, d_off, unsigned long long, "pc_offsets", blocks);
+    CTB_CUDA(ctx, cudaMemcpyAsync(d_vol, vol, total * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CTB_LAUNCH(ctx, launch_point_count(d_vol, total, threshold, d_cnt, blocks, ctx->stream));
+    std::vector<unsigned> cnt(blocks);
+    std::vector<unsigned long long> off(blocks);
+    CTB_CUDA(ctx, cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(unsigned) * blocks, cudaMemcpyDeviceToHost, ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    unsigned long long run = 0;
+    for (int b = 0; b < blocks; ++b) { off[b] = run; run += cnt[b]; }
+    *count = static_cast<int64_t>(run);
+    const long long keep = std::min<long long>(static_cast<long long>(run), capacity);
+    if (keep > 0) {
+        CTB_WS(ctx, d_pts, float4, "pc_points", keep);
+        CTB_CUDA(ctx, cudaMemcpyAsync(d_off, off.data(), sizeof(unsigned long long) * blocks, cudaMemcpyHostToDevice, ctx->stream));
+        CTB_LAUNCH(ctx, launch_point_write(d_vol, nx, ny, total, threshold, d_off, blocks, d_pts, keep, ctx->stream));
+        CTB_CUDA(ctx, cudaMemcpyAsync(points, d_pts, sizeof(float4) * keep, cudaMemcpyDeviceToHost, ctx->stream));
+        CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    return CTB_OK;
+}
+
+}  // extern "C"

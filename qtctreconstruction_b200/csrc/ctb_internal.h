@@ -1,0 +1,114 @@
+// ctb_internal.h — shared declarations of libctb200.so (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ctb200.h"
+
+namespace ctb {
+
+// ----------------------------------------------------------------- geometry
+// Padded detector geometry of reconstructSlice (SerialBackend.cpp:152-163).
+struct PadGeom {
+    int bins = 0;  // detector bins of the input sinogram
+    int sq = 0;    // square_bins = ceil(sqrt(2) * bins)
+    int pad = 0;   // pad_before = sq/2 - bins/2
+    int L = 0;     // fft_size = max(64, nextPow2(2 * sq))
+};
+PadGeom pad_geometry(int bins);
+
+// Layout of the filtered rows the backprojector reads: for each group of four
+// slices and each angle, `pitch` bins of float4 (one float per slice), with
+// `guard` zero bins in front of bin 0 so that every staged window lies inside
+// the row.
+struct FiltLayout {
+    int sq = 0;
+    int guard = 0;
+    int pitch = 0;
+};
+constexpr int kBpTile = 32;      // backprojection tile edge (voxels)
+constexpr int kBpWindow = 52;    // bins staged per angle and tile (>= 31*sqrt(2) + margins)
+FiltLayout filt_layout(int sq, int n_out);
+
+// FilterDesign (FilterDesign.cpp:13-111) in double precision: fft_size/2+1 values.
+std::vector<double> filter_response(int L, int type);
+
+// ----------------------------------------------------------- device buffer
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+// Kernel launchers (implemented in the .cu files). Each returns the CUDA error
+// of the launch.
+struct TrigTables {
+    const double2* d_cs = nullptr;  // (cos, sin) per angle in double
+    int na = 0;
+};
+
+cudaError_t launch_trig(const float* d_angles_deg, int na, double2* d_cs, cudaStream_t st);
+cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4* d_stats,
+                               cudaStream_t st);
+cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
+                             float4* d_img, float4* d_imgT, cudaStream_t st);
+cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
+                           int na, int nd, const double2* d_cs, float* d_sino, cudaStream_t st);
+cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
+                          const FiltLayout& fl, const float* d_Hs, const float2* d_tw,
+                          const float4* d_stats, int denorm, float scale, float4* d_filt,
+                          cudaStream_t st);
+cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltLayout& fl,
+                               int n_out, const double2* d_cs, const float4* d_stats,
+                               int denorm, float* d_out, unsigned* d_err, cudaStream_t st);
+cudaError_t launch_point_count(const float* d_vol, long long total, float thr,
+                               unsigned* d_block_counts, int blocks, cudaStream_t st);
+cudaError_t launch_point_write(const float* d_vol, int nx, int ny, long long total, float thr,
+                               const unsigned long long* d_block_offsets, int blocks,
+                               float4* d_points, long long cap, cudaStream_t st);
+int point_blocks(long long total);
+
+// Number of kernel launches one launcher issues (for the launch counter).
+constexpr int kFilterLaunches = 1;
+
+}  // namespace ctb
+
+// ------------------------------------------------------------------ context
+struct ctb_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::recursive_mutex mu;
+    std::string last_error;
+    uint64_t launches = 0;
+    double last_sino_ms = 0.0;
+    double last_recon_ms = 0.0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    // Named workspaces, grown on demand and kept until destruction.
+    std::map<std::string, ctb::DevBuf> ws;
+    // Cached tables: filter spectra per (L, type), twiddles per L.
+    std::map<std::pair<int, int>, ctb::DevBuf> filters;
+    std::map<int, ctb::DevBuf> twiddles;
+    // Angle tables: uniform angle sets per count; the last explicit list.
+    std::map<int, ctb::DevBuf> trig_uniform;
+    std::vector<float> user_angles;
+    unsigned* d_err = nullptr;  // device error word for bounded waits
+
+    // Stage profiling: a ring of event sets, one set per volume reconstruction.
+    static constexpr int kProfRing = 256;
+    static constexpr int kProfEvents = 5;
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_ev;  // kProfRing * kProfEvents
+    long long prof_calls = 0;
+};
+
+namespace ctb {
+// Get (or grow) a named device workspace of at least `bytes` bytes.
+void* workspace(ctb_ctx* ctx, const std::string& name, size_t bytes);
+}

@@ -1,0 +1,225 @@
+// forward.cu — angle tables, per-slice statistics, normalisation and the
+// ray-driven forward projector (RadonTransform stage of the FBP path).
+//
+// The reference's forward projector (SerialBackend::computeSinogram,
+// SerialBackend.cpp:59-136) splats every non-zero pixel onto the two detector
+// bins around s = (x-cx)cos + (y-cy)sin + floor(nd/2) with linear weights.
+// Here the same linear operator is evaluated as a gather: each thread owns one
+// detector bin (a ray) of one angle for four slices and walks the ray through
+// the image, collecting the pixels whose splat reaches its bin with the tent
+// weight 1 - |s - b| (the identical weights (1-frac, frac) of the splat). The
+// reference's edge rules are kept: bin 0 takes nothing from pixels with s < 0
+// and bin nd-1 takes the full value from pixels with s in [nd-1, nd).
+// Sinogram stores are coalesced by detector bin.
+#include <cfloat>
+#include <cmath>
+
+#include "ctb_internal.h"
+
+namespace ctb {
+namespace {
+
+// ------------------------------------------------------------------ trig
+// cos/sin of the angle in double precision: theta/pi = deg/180 exactly
+// representable as a double quotient; sincospi avoids the pi rounding.
+__global__ void k_trig(const float* __restrict__ deg, int na, double2* __restrict__ cs) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= na) return;
+    double s, c;
+    sincospi(static_cast<double>(deg[a]) / 180.0, &s, &c);
+    cs[a] = make_double2(c, s);
+}
+
+// ------------------------------------------------------------ slice stats
+// stats[z] = {min, max, span_fwd, span_denorm} (SerialBackend.cpp:70-80, 298-300).
+__global__ void __launch_bounds__(1024) k_slice_stats(const float* __restrict__ vol, long long npx,
+                                                      float4* __restrict__ stats) {
+    const int z = blockIdx.x;
+    const float* p = vol + static_cast<long long>(z) * npx;
+    float lo = FLT_MAX, hi = -FLT_MAX;
+    if ((npx & 3) == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+        const float4* p4 = reinterpret_cast<const float4*>(p);
+        for (long long i = threadIdx.x; i < npx / 4; i += blockDim.x) {
+            const float4 v = __ldg(p4 + i);
+            lo = fminf(lo, fminf(fminf(v.x, v.y), fminf(v.z, v.w)));
+            hi = fmaxf(hi, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+        }
+    } else {
+        for (long long i = threadIdx.x; i < npx; i += blockDim.x) {
+            const float v = __ldg(p + i);
+            lo = fminf(lo, v);
+            hi = fmaxf(hi, v);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    __shared__ float slo[32], shi[32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { slo[w] = lo; shi[w] = hi; }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        lo = l < nw ? slo[l] : FLT_MAX;
+        hi = l < nw ? shi[l] : -FLT_MAX;
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (l == 0) {
+            const float span = __fsub_rn(hi, lo);
+            stats[z] = make_float4(lo, hi, span < 1e-6f ? 1.0f : span, span <= 0.0f ? 1.0f : span);
+        }
+    }
+}
+
+// --------------------------------------------------------------- normalise
+// img[zg][y][x] = (v(4zg), v(4zg+1), v(4zg+2), v(4zg+3)) and imgT[zg][x][y], with
+// v = (raw - min) * (1 / span_fwd) for raw != 0 and v = 0 for raw == 0: the
+// reference skips background pixels (SerialBackend.cpp:104-106).
+__global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol, int w, int h, int nz,
+                                                   const float4* __restrict__ stats,
+                                                   float4* __restrict__ img, float4* __restrict__ imgT) {
+    __shared__ float4 tile[32][33];
+    const int zg = blockIdx.z;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    float lo[4], inv[4];
+    bool live[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int z = 4 * zg + j;
+        live[j] = z < nz;
+        const float4 st = live[j] ? stats[z] : make_float4(0.f, 0.f, 1.f, 1.f);
+        lo[j] = st.x;
+        inv[j] = __fdiv_rn(1.0f, st.z);
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int y = y0 + ty + 8 * r, x = x0 + tx;
+        float v[4] = {0.f, 0.f, 0.f, 0.f};
+        if (x < w && y < h) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (!live[j]) continue;
+                const float raw = __ldg(vol + (static_cast<long long>(4 * zg + j) * h + y) * w + x);
+                v[j] = (raw == 0.0f) ? 0.0f : __fmul_rn(__fsub_rn(raw, lo[j]), inv[j]);
+            }
+        }
+        const float4 q = make_float4(v[0], v[1], v[2], v[3]);
+        tile[ty + 8 * r][tx] = q;
+        if (x < w && y < h) img[(static_cast<long long>(zg) * h + y) * w + x] = q;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int x = x0 + ty + 8 * r, y = y0 + tx;
+        if (x < w && y < h) imgT[(static_cast<long long>(zg) * w + x) * h + y] = tile[tx][ty + 8 * r];
+    }
+}
+
+// ----------------------------------------------------------------- forward
+// One thread per (bin b, angle a, group of four slices). The ray is walked
+// along the image axis it is closest to (rows when |cos| >= |sin|, else
+// columns through the transposed copy), so each step crosses at most three
+// pixels of the minor axis. Per step, the crossing point is computed in
+// double precision (q* = q0 + p * dq, one FMA) and the tent weights of the
+// candidate pixels in float from the small offset (q - q*).
+__global__ void __launch_bounds__(128) k_forward(const float4* __restrict__ img,
+                                                 const float4* __restrict__ imgT, int w, int h,
+                                                 int nz, int na, int nd,
+                                                 const double2* __restrict__ cs,
+                                                 float* __restrict__ sino) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = blockIdx.y;
+    const int zg = blockIdx.z;
+    if (b >= nd) return;
+    const double2 t = cs[a];
+    const double c = t.x, s = t.y;
+    const bool rows = fabs(c) >= fabs(s);
+    const float4* base = rows ? img : imgT;
+    const int np = rows ? h : w;  // extent of the walked (major) axis
+    const int nq = rows ? w : h;  // extent of the gathered (minor) axis
+    const double kq = rows ? c : s;
+    const double kp = rows ? s : c;
+    const double cq = rows ? 0.5 * (w - 1) : 0.5 * (h - 1);
+    const double cp = rows ? 0.5 * (h - 1) : 0.5 * (w - 1);
+    const double dcf = static_cast<double>(nd / 2);
+    // s(q, p) = (q - cq) kq + (p - cp) kp + dcf;  s = b  <=>  q = q0 + p dq
+    const double inv = 1.0 / kq;
+    const double q0 = cq + (static_cast<double>(b) - dcf + cp * kp) * inv;
+    const double dq = -kp * inv;
+    const float kqf = static_cast<float>(kq);
+    const double reach = fabs(inv) + 1.0;  // |q - q*| < 1/|kq| contributes
+    // p range whose crossing point lies within [-reach, nq - 1 + reach]
+    int p_lo = 0, p_hi = np - 1;
+    if (dq != 0.0) {
+        double pa = (-reach - q0) / dq, pb = (nq - 1 + reach - q0) / dq;
+        if (pa > pb) { const double tmp = pa; pa = pb; pb = tmp; }
+        p_lo = max(0, static_cast<int>(floor(pa)) - 1);
+        p_hi = min(np - 1, static_cast<int>(ceil(pb)) + 1);
+    } else if (q0 < -reach || q0 > nq - 1 + reach) {
+        p_hi = -1;
+    }
+    const bool first = (b == 0), last = (b == nd - 1);
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4* plane = base + static_cast<long long>(zg) * np * nq;
+    for (int p = p_lo; p <= p_hi; ++p) {
+        const double qs = fma(static_cast<double>(p), dq, q0);
+        const double qf = floor(qs);
+        const int qi = static_cast<int>(qf);
+        const float d0 = static_cast<float>(qs - qf);  // in [0, 1)
+        const float4* row = plane + static_cast<long long>(p) * nq;
+#pragma unroll
+        for (int k = -1; k <= 2; ++k) {
+            const int q = qi + k;
+            const float tt = (static_cast<float>(k) - d0) * kqf;  // s - b for pixel q
+            float wgt = 1.0f - fabsf(tt);
+            if (first && tt < 0.0f) wgt = 0.0f;
+            if (last && tt >= 0.0f && tt < 1.0f) wgt = 1.0f;
+            if (wgt > 0.0f && q >= 0 && q < nq) {
+                const float4 v = __ldg(row + q);
+                acc.x = fmaf(wgt, v.x, acc.x);
+                acc.y = fmaf(wgt, v.y, acc.y);
+                acc.z = fmaf(wgt, v.z, acc.z);
+                acc.w = fmaf(wgt, v.w, acc.w);
+            }
+        }
+    }
+    const float r[4] = {acc.x, acc.y, acc.z, acc.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int z = 4 * zg + j;
+        if (z < nz) sino[(static_cast<long long>(z) * na + a) * nd + b] = r[j];
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_trig(const float* d_angles_deg, int na, double2* d_cs, cudaStream_t st) {
+    k_trig<<<(na + 127) / 128, 128, 0, st>>>(d_angles_deg, na, d_cs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4* d_stats,
+                               cudaStream_t st) {
+    k_slice_stats<<<nz, 1024, 0, st>>>(d_vol, npx, d_stats);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
+                             float4* d_img, float4* d_imgT, cudaStream_t st) {
+    const dim3 grid((w + 31) / 32, (h + 31) / 32, (nz + 3) / 4);
+    k_normalize<<<grid, 256, 0, st>>>(d_vol, w, h, nz, d_stats, d_img, d_imgT);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
+                           int na, int nd, const double2* d_cs, float* d_sino, cudaStream_t st) {
+    const dim3 grid((nd + 127) / 128, na, (nz + 3) / 4);
+    k_forward<<<grid, 128, 0, st>>>(d_img, d_imgT, w, h, nz, na, nd, d_cs, d_sino);
+    return cudaGetLastError();
+}
+
+}  // namespace ctb
