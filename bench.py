@@ -238,7 +238,9 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
     nd = odd_nd(n)
     updates = n * n * nz * na
     be = ctb.B200Backend(local)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-legacy) stream: the library and the timing events share it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     be.set_stream(stream.cuda_stream)
     be.set_profiling(True)
 

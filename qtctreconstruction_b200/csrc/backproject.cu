@@ -76,12 +76,15 @@ struct AngleRec {
     float f0;  // tile-origin u minus window start
     float c, s;
     int ws;    // window start bin (unguarded coordinates)
+    float cf, sf;  // the reference's float cos/sin (edge decisions only)
+    int edge;      // the window reaches a detector edge: decide taps like the reference
+    int pad;
 };
 
 __global__ void __launch_bounds__(THREADS) k_backproject(
     const float4* __restrict__ filt, int nz, int na, int sq, int guard, int pitch, int n,
-    const double2* __restrict__ cs, const float4* __restrict__ stats, int denorm,
-    float* __restrict__ out, unsigned* __restrict__ err) {
+    Trig trig, const float4* __restrict__ stats, int denorm, float* __restrict__ out,
+    unsigned* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     auto win = reinterpret_cast<float4 (*)[CA][WIN]>(smem_raw);
     auto rec = reinterpret_cast<AngleRec (*)[CA]>(smem_raw + sizeof(float4) * NBUF * CA * WIN);
@@ -130,6 +133,7 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
     __syncthreads();
 
     const double dcd = static_cast<double>(sq / 2);
+    const float dcf = static_cast<float>(sq / 2);
     const double ox = static_cast<double>(x0 - rad), oy = static_cast<double>(y0 - rad);
     const float4* plane = filt + static_cast<long long>(zg) * na * pitch;
     const int nch = (na + CA - 1) / CA;
@@ -139,15 +143,22 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
         const int cnt = min(CA, na - a0);
         if (t < cnt) {
             const int a = a0 + t;
-            const double2 tc = cs[a];
+            const double2 tc = trig.cs[a];
+            const float2 tf = trig.csf[a];
             const double uo = ox * tc.x - oy * tc.y + dcd;
             const double umin = uo + fmin(0.0, (TILE - 1) * tc.x) + fmin(0.0, -(TILE - 1) * tc.y);
+            const double umax = uo + fmax(0.0, (TILE - 1) * tc.x) + fmax(0.0, -(TILE - 1) * tc.y);
             const int ws = static_cast<int>(floor(umin)) - 1;
             AngleRec r;
             r.f0 = static_cast<float>(uo - ws);
             r.c = static_cast<float>(tc.x);
             r.s = static_cast<float>(tc.y);
             r.ws = ws;
+            r.cf = tf.x;
+            r.sf = tf.y;
+            // taps near bin 0 or bin sq-1: the reference's float u decides them
+            r.edge = (umin < 2.0 || umax > sq - 3.0) ? 1 : 0;
+            r.pad = 0;
             rec[b][t] = r;
             bulk_load(&win[b][t][0], plane + static_cast<long long>(a) * pitch + guard + ws,
                       WIN * sizeof(float4), &bar[b]);
@@ -175,21 +186,43 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
             const float4* w = win[b][j];
             const float ub = fmaf(fx, r.c, fmaf(-fy, r.s, r.f0));
             const float c8 = 8.0f * r.c;
+            if (!r.edge) {
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const float u = fmaf(static_cast<float>(k), c8, ub);
-                const float fl = floorf(u);
-                const int i = static_cast<int>(fl);
-                const float fr = u - fl;
-                const int gi = r.ws + i;
-                const bool ok = (gi >= 0) && (gi + 1 < sq);
-                const float w1 = ok ? fr : 0.0f;
-                const float w0 = ok ? 1.0f - fr : 0.0f;
-                const float4 lo = w[i], hi = w[i + 1];
-                acc[k].x = fmaf(w1, hi.x, fmaf(w0, lo.x, acc[k].x));
-                acc[k].y = fmaf(w1, hi.y, fmaf(w0, lo.y, acc[k].y));
-                acc[k].z = fmaf(w1, hi.z, fmaf(w0, lo.z, acc[k].z));
-                acc[k].w = fmaf(w1, hi.w, fmaf(w0, lo.w, acc[k].w));
+                for (int k = 0; k < 4; ++k) {
+                    const float u = fmaf(static_cast<float>(k), c8, ub);
+                    const float fl = floorf(u);
+                    const int i = static_cast<int>(fl);
+                    const float w1 = u - fl;
+                    const float w0 = 1.0f - w1;
+                    const float4 lo = w[i], hi = w[i + 1];
+                    acc[k].x = fmaf(w1, hi.x, fmaf(w0, lo.x, acc[k].x));
+                    acc[k].y = fmaf(w1, hi.y, fmaf(w0, lo.y, acc[k].y));
+                    acc[k].z = fmaf(w1, hi.z, fmaf(w0, lo.z, acc[k].z));
+                    acc[k].w = fmaf(w1, hi.w, fmaf(w0, lo.w, acc[k].w));
+                }
+            } else {
+                // SerialBackend.cpp:229-239 evaluates u = (xx cos - yy sin) + dc in
+                // float without fused multiply-add and keeps the tap pair only when
+                // 0 <= floor(u) and floor(u) + 1 < sq; that decision is reproduced
+                // here exactly, the interpolation itself uses the accurate u.
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float u = fmaf(static_cast<float>(k), c8, ub);
+                    const float fl = floorf(u);
+                    const int i = static_cast<int>(fl);
+                    const float xs = static_cast<float>(x0 + lx + 8 * k - rad);
+                    const float ys = static_cast<float>(y0 + ly - rad);
+                    const float us = __fadd_rn(__fsub_rn(__fmul_rn(xs, r.cf), __fmul_rn(ys, r.sf)), dcf);
+                    const int is = static_cast<int>(floorf(us));
+                    const bool ok = (is >= 0) && (is + 1 < sq);
+                    const float w1 = ok ? u - fl : 0.0f;
+                    const float w0 = ok ? 1.0f - (u - fl) : 0.0f;
+                    const float4 lo = w[i], hi = w[i + 1];
+                    acc[k].x = fmaf(w1, hi.x, fmaf(w0, lo.x, acc[k].x));
+                    acc[k].y = fmaf(w1, hi.y, fmaf(w0, lo.y, acc[k].y));
+                    acc[k].z = fmaf(w1, hi.z, fmaf(w0, lo.z, acc[k].z));
+                    acc[k].w = fmaf(w1, hi.w, fmaf(w0, lo.w, acc[k].w));
+                }
             }
         }
         if (!__syncthreads_and(landed)) { ok_all = false; break; }
@@ -235,16 +268,16 @@ FiltLayout filt_layout(int sq, int n_out) {
 }
 
 cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltLayout& fl,
-                               int n_out, const double2* d_cs, const float4* d_stats,
-                               int denorm, float* d_out, unsigned* d_err, cudaStream_t st) {
+                               int n_out, Trig trig, const float4* d_stats, int denorm,
+                               float* d_out, unsigned* d_err, cudaStream_t st) {
     const dim3 grid((n_out + TILE - 1) / TILE, (n_out + TILE - 1) / TILE, (nz + 3) / 4);
     const size_t smem = sizeof(float4) * NBUF * CA * WIN + sizeof(AngleRec) * NBUF * CA +
                         sizeof(unsigned long long) * NBUF;
     const cudaError_t e = cudaFuncSetAttribute(
         k_backproject, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    k_backproject<<<grid, THREADS, smem, st>>>(d_filt, nz, na, fl.sq, fl.guard, fl.pitch, n_out, d_cs,
-                                            d_stats, denorm, d_out, d_err);
+    k_backproject<<<grid, THREADS, smem, st>>>(d_filt, nz, na, fl.sq, fl.guard, fl.pitch, n_out, trig,
+                                               d_stats, denorm, d_out, d_err);
     return cudaGetLastError();
 }
 

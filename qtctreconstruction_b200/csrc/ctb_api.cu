@@ -101,38 +101,56 @@ std::vector<float> uniform_angles(int na) {
     return a;
 }
 
-// cos/sin table (double) of the angles on the device. Uniform angles
-// (angles_deg == NULL, 180/na * a in float) are cached per count; an explicit
-// angle list is re-uploaded only when it differs from the previous one.
-ctb_status trig_table(ctb_ctx* ctx, const float* angles_deg, int na, const double2** out) {
+// Fill a device angle table: na double2 (device sincospi) followed by na
+// float2 holding the reference's float cos/sin of degToRad(deg)
+// (SerialBackend.cpp:92-95, 198-204; Utils.cpp:44-46), computed here on the
+// host with the same libm calls.
+ctb_status fill_trig(ctb_ctx* ctx, const float* angles_deg, int na, void* table) {
+    std::vector<float2> csf(na);
+    for (int a = 0; a < na; ++a) {
+        const float th = angles_deg[a] * 3.14159265358979323846f / 180.0f;
+        csf[a] = make_float2(std::cos(th), std::sin(th));
+    }
+    float* d_deg = static_cast<float*>(workspace(ctx, "angles_upload", sizeof(float) * na));
+    if (!d_deg) return fail(ctx, CTB_ERR_OOM, "angle upload buffer");
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // previous users of the buffers are done
+    CTB_CUDA(ctx, cudaMemcpy(d_deg, angles_deg, sizeof(float) * na, cudaMemcpyHostToDevice));
+    CTB_CUDA(ctx, cudaMemcpy(static_cast<double2*>(table) + na, csf.data(), sizeof(float2) * na,
+                             cudaMemcpyHostToDevice));
+    CTB_LAUNCH(ctx, launch_trig(d_deg, na, static_cast<double2*>(table), ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return CTB_OK;
+}
+
+// Angle tables on the device. Uniform angles (angles_deg == NULL: 180/na * a
+// in float) are cached per count; an explicit angle list is re-uploaded only
+// when it differs from the previous one.
+ctb_status trig_table(ctb_ctx* ctx, const float* angles_deg, int na, Trig* out) {
+    const size_t bytes = (sizeof(double2) + sizeof(float2)) * na;
+    void* table = nullptr;
     if (!angles_deg) {
         auto it = ctx->trig_uniform.find(na);
         if (it == ctx->trig_uniform.end()) {
             const std::vector<float> uni = uniform_angles(na);
-            DevBuf deg, cs;
-            CTB_CUDA(ctx, cudaMalloc(&deg.ptr, sizeof(float) * na));
-            CTB_CUDA(ctx, cudaMalloc(&cs.ptr, sizeof(double2) * na));
-            CTB_CUDA(ctx, cudaMemcpy(deg.ptr, uni.data(), sizeof(float) * na, cudaMemcpyHostToDevice));
-            CTB_LAUNCH(ctx, launch_trig(static_cast<float*>(deg.ptr), na, static_cast<double2*>(cs.ptr),
-                                        ctx->stream));
-            CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-            cudaFree(deg.ptr);
-            cs.bytes = sizeof(double2) * na;
-            it = ctx->trig_uniform.emplace(na, cs).first;
+            DevBuf b;
+            CTB_CUDA(ctx, cudaMalloc(&b.ptr, bytes));
+            b.bytes = bytes;
+            it = ctx->trig_uniform.emplace(na, b).first;
+            CTB_TRY(fill_trig(ctx, uni.data(), na, b.ptr));
         }
-        *out = static_cast<const double2*>(it->second.ptr);
-        return CTB_OK;
+        table = it->second.ptr;
+    } else {
+        table = workspace(ctx, "trig_user", bytes);
+        if (!table) return fail(ctx, CTB_ERR_OOM, "angle table");
+        if (ctx->user_angles.size() != static_cast<size_t>(na) ||
+            std::memcmp(ctx->user_angles.data(), angles_deg, sizeof(float) * na) != 0) {
+            ctx->user_angles.clear();
+            CTB_TRY(fill_trig(ctx, angles_deg, na, table));
+            ctx->user_angles.assign(angles_deg, angles_deg + na);
+        }
     }
-    CTB_WS(ctx, d_cs, double2, "trig_user", na);
-    if (ctx->user_angles.size() != static_cast<size_t>(na) ||
-        std::memcmp(ctx->user_angles.data(), angles_deg, sizeof(float) * na) != 0) {
-        CTB_WS(ctx, d_deg, float, "angles_user", na);
-        CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // previous users of the table are done
-        CTB_CUDA(ctx, cudaMemcpy(d_deg, angles_deg, sizeof(float) * na, cudaMemcpyHostToDevice));
-        CTB_LAUNCH(ctx, launch_trig(d_deg, na, d_cs, ctx->stream));
-        ctx->user_angles.assign(angles_deg, angles_deg + na);
-    }
-    *out = d_cs;
+    out->cs = static_cast<const double2*>(table);
+    out->csf = reinterpret_cast<const float2*>(static_cast<const double2*>(table) + na);
     return CTB_OK;
 }
 
@@ -204,12 +222,13 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     const size_t img = static_cast<size_t>(nzg) * w * h;
     CTB_WS(ctx, d_img, float4, "img", img);
     CTB_WS(ctx, d_imgT, float4, "imgT", img);
-    const double2* d_cs = nullptr;
-    CTB_TRY(trig_table(ctx, angles_deg, na, &d_cs));
+    Trig trig;
+    CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
     CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream));
     CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream));
     mark(ctx, ev, 1);
-    CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd, d_cs, d_sino, ctx->stream));
+    CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd, trig, d_sino, ctx->d_err,
+                                   ctx->stream));
     return CTB_OK;
 }
 
@@ -225,14 +244,14 @@ ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins
     const float* d_Hs = nullptr;
     const float2* d_tw = nullptr;
     CTB_TRY(filter_tables(ctx, g.L, filter, &d_Hs, &d_tw));
-    const double2* d_cs = nullptr;
-    CTB_TRY(trig_table(ctx, angles_deg, na, &d_cs));
+    Trig trig;
+    CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
     // SerialBackend.cpp:246: pi / (2 na) in float
     const float scale = 3.14159265358979323846f / (2.0f * static_cast<float>(na));
     CTB_LAUNCH(ctx, launch_filter(d_sino, nz, na, g, fl, d_Hs, d_tw, d_stats, denorm, scale, d_filt,
                                   ctx->stream));
     mark(ctx, ev, 3);
-    CTB_LAUNCH(ctx, launch_backproject(d_filt, nz, na, fl, n_out, d_cs, d_stats, denorm, d_out,
+    CTB_LAUNCH(ctx, launch_backproject(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out,
                                        ctx->d_err, ctx->stream));
     return CTB_OK;
 }

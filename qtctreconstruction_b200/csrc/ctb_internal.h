@@ -45,27 +45,34 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
-// Kernel launchers (implemented in the .cu files). Each returns the CUDA error
-// of the launch.
-struct TrigTables {
-    const double2* d_cs = nullptr;  // (cos, sin) per angle in double
-    int na = 0;
+// Angle tables on the device.
+//   cs:  (cos, sin) in double precision of theta = deg * pi / 180 (sincospi),
+//        the values every interpolation weight is computed from;
+//   csf: the reference's own float (cos, sin) of degToRad(deg) (Utils.cpp:44-46
+//        with libm cosf/sinf), used only to reproduce its discontinuous
+//        decisions (which taps exist at the detector edges) bit for bit.
+struct Trig {
+    const double2* cs = nullptr;
+    const float2* csf = nullptr;
 };
 
+// Kernel launchers (implemented in the .cu files). Each returns the CUDA error
+// of the launch.
 cudaError_t launch_trig(const float* d_angles_deg, int na, double2* d_cs, cudaStream_t st);
 cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4* d_stats,
                                cudaStream_t st);
 cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
                              float4* d_img, float4* d_imgT, cudaStream_t st);
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
-                           int na, int nd, const double2* d_cs, float* d_sino, cudaStream_t st);
+                           int na, int nd, Trig trig, float* d_sino, unsigned* d_err,
+                           cudaStream_t st);
 cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
                           const FiltLayout& fl, const float* d_Hs, const float2* d_tw,
                           const float4* d_stats, int denorm, float scale, float4* d_filt,
                           cudaStream_t st);
 cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltLayout& fl,
-                               int n_out, const double2* d_cs, const float4* d_stats,
-                               int denorm, float* d_out, unsigned* d_err, cudaStream_t st);
+                               int n_out, Trig trig, const float4* d_stats, int denorm,
+                               float* d_out, unsigned* d_err, cudaStream_t st);
 cudaError_t launch_point_count(const float* d_vol, long long total, float thr,
                                unsigned* d_block_counts, int blocks, cudaStream_t st);
 cudaError_t launch_point_write(const float* d_vol, int nx, int ny, long long total, float thr,

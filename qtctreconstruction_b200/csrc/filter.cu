@@ -154,17 +154,102 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int L, int Ns, int ti
     __syncthreads();
 }
 
-template <bool INV, int K>
-__device__ void fft(float2* buf, int L, int logL, int tid, int T, const float2* __restrict__ tw) {
-    int Ns = 1;
+// First forward pass (Ns = 1): the inputs come straight from the two sinogram
+// rows (zero outside [pad, pad + nd)), so the zero-padded sequence is never
+// materialised.
+template <int R, int K>
+__device__ __forceinline__ void first_pass(float2* buf, int L, int tid, int T, const float* r0,
+                                           const float* r1, int pad, int nd) {
+    constexpr int NB = 16 * K / R;
+    float2 v[NB][R];
+    const int LR = L / R;
+#pragma unroll
+    for (int bi = 0; bi < NB; ++bi) {
+        const int j = tid + bi * T;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = j + r * LR - pad;
+            const bool in = i >= 0 && i < nd;
+            v[bi][r] = make_float2(in && r0 ? __ldg(r0 + i) : 0.0f, in && r1 ? __ldg(r1 + i) : 0.0f);
+        }
+        dft<R, false>(v[bi]);
+    }
+#pragma unroll
+    for (int bi = 0; bi < NB; ++bi) {
+        const int j = tid + bi * T;
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[padi(j * R + r)] = v[bi][r];
+    }
+    __syncthreads();
+}
+
+// The forward transform's last radix-16 pass (Ns = L/16) leaves spectrum bin
+// j + r L/16 in register r of butterfly j -- exactly the inputs of the inverse
+// transform's first radix-16 pass (Ns = 1). Both passes and the filter
+// multiply between them run in registers.
+template <int K>
+__device__ __forceinline__ void fused_middle(float2* buf, int L, int tid, int T,
+                                             const float2* __restrict__ tw,
+                                             const float* __restrict__ Hs) {
+    constexpr int NB = K;
+    float2 v[NB][16];
+    const int LR = L / 16;
+#pragma unroll
+    for (int bi = 0; bi < NB; ++bi) {
+        const int j = tid + bi * T;
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[bi][r] = buf[padi(j + r * LR)];
+        if (LR > 1) {
+#pragma unroll
+            for (int r = 1; r < 16; ++r) v[bi][r] = cmul(v[bi][r], __ldg(tw + r * j));
+        }
+        dft16<false>(v[bi]);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const float hk = __ldg(Hs + j + r * LR);
+            v[bi][r].x *= hk;
+            v[bi][r].y *= hk;
+        }
+        dft16<true>(v[bi]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int bi = 0; bi < NB; ++bi) {
+        const int j = tid + bi * T;
+#pragma unroll
+        for (int r = 0; r < 16; ++r) buf[padi(j * 16 + r)] = v[bi][r];
+    }
+    __syncthreads();
+}
+
+// Filter one complex row pair in shared memory: forward FFT, Hs multiply,
+// inverse FFT (natural order out). Radix-16 passes around the fused middle; the
+// radix-2/4/8 remainder pass runs first in the forward and last in the inverse.
+template <int K>
+__device__ void filter_rows(float2* buf, int L, int logL, int tid, int T, const float* r0,
+                            const float* r1, int pad, int nd, const float2* __restrict__ tw,
+                            const float* __restrict__ Hs) {
     const int rem = logL & 3;
-    if (rem == 1) { stockham_pass<2, INV, K>(buf, L, Ns, tid, T, tw); Ns *= 2; }
-    else if (rem == 2) { stockham_pass<4, INV, K>(buf, L, Ns, tid, T, tw); Ns *= 4; }
-    else if (rem == 3) { stockham_pass<8, INV, K>(buf, L, Ns, tid, T, tw); Ns *= 8; }
-    for (int p = 0; p < (logL >> 2); ++p) {
-        stockham_pass<16, INV, K>(buf, L, Ns, tid, T, tw);
+    const int q = logL >> 2;  // radix-16 passes per transform (>= 1 for L >= 64)
+    int Ns = 1;
+    if (rem == 1) { first_pass<2, K>(buf, L, tid, T, r0, r1, pad, nd); Ns = 2; }
+    else if (rem == 2) { first_pass<4, K>(buf, L, tid, T, r0, r1, pad, nd); Ns = 4; }
+    else if (rem == 3) { first_pass<8, K>(buf, L, tid, T, r0, r1, pad, nd); Ns = 8; }
+    else { first_pass<16, K>(buf, L, tid, T, r0, r1, pad, nd); Ns = 16; }
+    const int fwd16 = q - 1 - (rem == 0 ? 1 : 0);  // radix-16 passes between first and middle
+    for (int p = 0; p < fwd16; ++p) {
+        stockham_pass<16, false, K>(buf, L, Ns, tid, T, tw);
         Ns *= 16;
     }
+    fused_middle<K>(buf, L, tid, T, tw, Hs);
+    Ns = 16;
+    for (int p = 0; p < q - 1; ++p) {
+        stockham_pass<16, true, K>(buf, L, Ns, tid, T, tw);
+        Ns *= 16;
+    }
+    if (rem == 1) stockham_pass<2, true, K>(buf, L, Ns, tid, T, tw);
+    else if (rem == 2) stockham_pass<4, true, K>(buf, L, Ns, tid, T, tw);
+    else if (rem == 3) stockham_pass<8, true, K>(buf, L, Ns, tid, T, tw);
 }
 
 // Per-slice output scale: pi/(2 na) times the denormalisation span.
@@ -178,60 +263,36 @@ __device__ __forceinline__ float slice_scale(const float4* stats, int z, int nz,
     return span > 0.0f ? scale * span : 0.0f;  // OpenMP: span <= 0 -> min everywhere
 }
 
-// grid (na, nzg); block 2 * T threads with T = L / (16 K); dynamic smem
-// 2 * (L + L/16) float2. K = 1 up to L = 4096, K = 2 for L = 8192.
+// grid (na, ceil(nz/2)); block T = L/(16 K) threads filtering slices 2y and
+// 2y+1 at angle x; dynamic smem (L + L/16) float2.
 template <int K>
-__global__ void __launch_bounds__(512) k_filter(const float* __restrict__ sino, int nz, int na, int nd, int sq, int pad,
-                         int L, int logL, int guard, int pitch, const float* __restrict__ Hs,
-                         const float2* __restrict__ tw, const float4* __restrict__ stats,
-                         int denorm, float scale, float4* __restrict__ filt) {
+__global__ void __launch_bounds__(256) k_filter(const float* __restrict__ sino, int nz, int na, int nd,
+                                                int sq, int pad, int L, int logL, int guard, int pitch,
+                                                const float* __restrict__ Hs,
+                                                const float2* __restrict__ tw,
+                                                const float4* __restrict__ stats, int denorm,
+                                                float scale, float4* __restrict__ filt) {
     extern __shared__ float2 smem[];
-    const int a = blockIdx.x, zg = blockIdx.y;
-    const int T = L / (16 * K);
-    const int f = threadIdx.x / T;  // which of the two complex rows
-    const int tid = threadIdx.x - f * T;
-    const int lp = L + (L >> 4);
-    float2* buf = smem + f * lp;
-    // load rows (4zg + 2f) and (4zg + 2f + 1) as real and imaginary parts
-    const int z0 = 4 * zg + 2 * f, z1 = z0 + 1;
+    const int a = blockIdx.x;
+    const int z0 = 2 * blockIdx.y, z1 = z0 + 1;
+    const int T = blockDim.x;
+    const int tid = threadIdx.x;
     const float* r0 = sino + (static_cast<long long>(z0) * na + a) * nd;
-    const float* r1 = sino + (static_cast<long long>(z1) * na + a) * nd;
-    for (int i = tid; i < L; i += T) {
-        const int j = i - pad;
-        float re = 0.f, im = 0.f;
-        if (j >= 0 && j < nd) {
-            if (z0 < nz) re = __ldg(r0 + j);
-            if (z1 < nz) im = __ldg(r1 + j);
-        }
-        buf[padi(i)] = make_float2(re, im);
-    }
-    __syncthreads();
-    fft<false, K>(buf, L, logL, tid, T, tw);
-    for (int k = tid; k < L; k += T) {
-        const float h = __ldg(Hs + k);
-        float2 v = buf[padi(k)];
-        v.x *= h;
-        v.y *= h;
-        buf[padi(k)] = v;
-    }
-    __syncthreads();
-    fft<true, K>(buf, L, logL, tid, T, tw);
-    // write the first sq samples of all four rows as float4, guard bins as 0
-    const float s0 = slice_scale(stats, 4 * zg + 0, nz, denorm, scale);
-    const float s1 = slice_scale(stats, 4 * zg + 1, nz, denorm, scale);
-    const float s2 = slice_scale(stats, 4 * zg + 2, nz, denorm, scale);
-    const float s3 = slice_scale(stats, 4 * zg + 3, nz, denorm, scale);
-    const float2* b0 = smem;
-    const float2* b1 = smem + lp;
-    float4* dst = filt + (static_cast<long long>(zg) * na + a) * pitch;
-    for (int i = threadIdx.x; i < pitch; i += blockDim.x) {
+    const float* r1 = z1 < nz ? sino + (static_cast<long long>(z1) * na + a) * nd : nullptr;
+    filter_rows<K>(smem, L, logL, tid, T, r0, r1, pad, nd, tw, Hs);
+    const float s0 = slice_scale(stats, z0, nz, denorm, scale);
+    const float s1 = slice_scale(stats, z1, nz, denorm, scale);
+    // rows z0, z1 are lanes (z0 % 4, z0 % 4 + 1) of the float4 layout
+    float2* dst = reinterpret_cast<float2*>(filt + (static_cast<long long>(z0 / 4) * na + a) * pitch) +
+                  ((z0 & 3) >> 1);
+    for (int i = tid; i < pitch; i += T) {
         const int j = i - guard;
-        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+        float2 o = make_float2(0.f, 0.f);
         if (j >= 0 && j < sq) {
-            const float2 u = b0[padi(j)], v = b1[padi(j)];
-            o = make_float4(u.x * s0, u.y * s1, v.x * s2, v.y * s3);
+            const float2 u = smem[padi(j)];
+            o = make_float2(u.x * s0, u.y * s1);
         }
-        dst[i] = o;
+        dst[2 * i] = o;
     }
 }
 
@@ -244,13 +305,13 @@ cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
     int logL = 0;
     while ((1 << logL) < g.L) ++logL;
     const int K = g.L > 4096 ? 2 : 1;
-    const int threads = 2 * (g.L / (16 * K));
-    const size_t smem = 2 * static_cast<size_t>(g.L + (g.L >> 4)) * sizeof(float2);
+    const int threads = g.L / (16 * K);
+    const size_t smem = static_cast<size_t>(g.L + (g.L >> 4)) * sizeof(float2);
     auto kern = K == 2 ? k_filter<2> : k_filter<1>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    const dim3 grid(na, (nz + 3) / 4);
+    const dim3 grid(na, (nz + 1) / 2);
     kern<<<grid, threads, smem, st>>>(d_sino, nz, na, g.bins, g.sq, g.pad, g.L, logL, fl.guard,
                                       fl.pitch, d_Hs, d_tw, d_stats, denorm, scale, d_filt);
     return cudaGetLastError();

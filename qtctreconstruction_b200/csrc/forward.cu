@@ -120,77 +120,243 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
 }
 
 // ----------------------------------------------------------------- forward
-// One thread per (bin b, angle a, group of four slices). The ray is walked
+// A CTA owns FB = 128 consecutive detector bins (rays) of one angle and eight
+// slices (two float4 planes of the normalised image). The ray family is walked
 // along the image axis it is closest to (rows when |cos| >= |sin|, else
-// columns through the transposed copy), so each step crosses at most three
-// pixels of the minor axis. Per step, the crossing point is computed in
-// double precision (q* = q0 + p * dq, one FMA) and the tent weights of the
-// candidate pixels in float from the small offset (q - q*).
-__global__ void __launch_bounds__(128) k_forward(const float4* __restrict__ img,
-                                                 const float4* __restrict__ imgT, int w, int h,
-                                                 int nz, int na, int nd,
-                                                 const double2* __restrict__ cs,
-                                                 float* __restrict__ sino) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+// columns of the transposed copy), so every step crosses at most three pixels
+// of the gathered axis. Rows are processed in chunks of PCH = 8; per chunk the
+// row segments the CTA's rays can touch (FW pixels per row and plane) are
+// staged into shared memory by the bulk-copy engine, double-buffered on
+// mbarriers, with zeros where a segment leaves the image. The crossing point
+// q*(b, p) is evaluated in double once per chunk and split into an integer
+// and a float fraction; within the chunk each thread steps in float on small
+// numbers. The two edge rays (bins 0 and nd-1), where the reference's rules
+// are discontinuous, decide which pixels count with the reference's own float
+// arithmetic (SerialBackend.cpp:109-120).
+constexpr int FB = 128;   // rays per CTA
+constexpr int PCH = 8;    // walked rows per chunk
+constexpr int FW = 200;   // staged pixels per row and plane (>= 127 sqrt(2) + 7 + 8)
+constexpr int FNB = 2;    // chunk buffers
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
+                                          unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  unsigned* err) {
+    for (unsigned it = 0; it < (1u << 22); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (err) atomicOr(err, 2u);
+    return false;
+}
+
+__global__ void __launch_bounds__(FB) k_forward(const float4* __restrict__ img,
+                                                const float4* __restrict__ imgT, int w, int h,
+                                                int nz, int na, int nd, Trig trig,
+                                                float* __restrict__ sino, unsigned* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float4* seg = reinterpret_cast<float4*>(smem_raw);  // [FNB][2][PCH][FW]
+    auto bar = reinterpret_cast<unsigned long long*>(smem_raw + sizeof(float4) * FNB * 2 * PCH * FW);
+
     const int a = blockIdx.y;
-    const int zg = blockIdx.z;
-    if (b >= nd) return;
-    const double2 t = cs[a];
-    const double c = t.x, s = t.y;
+    const int b0 = blockIdx.x * FB;
+    const int b1 = min(b0 + FB, nd);  // exclusive
+    const int nzg = (nz + 3) / 4;
+    const int g0 = 2 * blockIdx.z;
+    const bool has_g1 = g0 + 1 < nzg;
+    const int t = threadIdx.x;
+    const int b = b0 + t;
+
+    const double2 tc = trig.cs[a];
+    const double c = tc.x, s = tc.y;
     const bool rows = fabs(c) >= fabs(s);
     const float4* base = rows ? img : imgT;
-    const int np = rows ? h : w;  // extent of the walked (major) axis
-    const int nq = rows ? w : h;  // extent of the gathered (minor) axis
+    const int np = rows ? h : w;  // walked axis
+    const int nq = rows ? w : h;  // gathered axis
     const double kq = rows ? c : s;
     const double kp = rows ? s : c;
     const double cq = rows ? 0.5 * (w - 1) : 0.5 * (h - 1);
     const double cp = rows ? 0.5 * (h - 1) : 0.5 * (w - 1);
     const double dcf = static_cast<double>(nd / 2);
-    // s(q, p) = (q - cq) kq + (p - cp) kp + dcf;  s = b  <=>  q = q0 + p dq
+    // s(q, p) = (q - cq) kq + (p - cp) kp + dcf = b  <=>  q = q0(b) + p dq
     const double inv = 1.0 / kq;
-    const double q0 = cq + (static_cast<double>(b) - dcf + cp * kp) * inv;
     const double dq = -kp * inv;
-    const float kqf = static_cast<float>(kq);
-    const double reach = fabs(inv) + 1.0;  // |q - q*| < 1/|kq| contributes
-    // p range whose crossing point lies within [-reach, nq - 1 + reach]
+    const double qb0 = cq + (static_cast<double>(b0) - dcf + cp * kp) * inv;
+    const double qb1 = cq + (static_cast<double>(b1 - 1) - dcf + cp * kp) * inv;
+    const double q0 = cq + (static_cast<double>(b) - dcf + cp * kp) * inv;
+    const double reach = fabs(inv) + 2.0;
+
+    // walked range touched by any of the CTA's rays (block-uniform)
     int p_lo = 0, p_hi = np - 1;
     if (dq != 0.0) {
-        double pa = (-reach - q0) / dq, pb = (nq - 1 + reach - q0) / dq;
-        if (pa > pb) { const double tmp = pa; pa = pb; pb = tmp; }
-        p_lo = max(0, static_cast<int>(floor(pa)) - 1);
-        p_hi = min(np - 1, static_cast<int>(ceil(pb)) + 1);
-    } else if (q0 < -reach || q0 > nq - 1 + reach) {
-        p_hi = -1;
+        double pa0 = (-reach - qb0) / dq, pb0 = (nq - 1 + reach - qb0) / dq;
+        double pa1 = (-reach - qb1) / dq, pb1 = (nq - 1 + reach - qb1) / dq;
+        const double lo = fmin(fmin(pa0, pb0), fmin(pa1, pb1));
+        const double hi = fmax(fmax(pa0, pb0), fmax(pa1, pb1));
+        p_lo = max(0, static_cast<int>(floor(lo)) - 1);
+        p_hi = min(np - 1, static_cast<int>(ceil(hi)) + 1);
+    } else {
+        const double qlo = fmin(qb0, qb1), qhi = fmax(qb0, qb1);
+        if (qhi < -reach || qlo > nq - 1 + reach) p_hi = -1;
     }
-    const bool first = (b == 0), last = (b == nd - 1);
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4* plane = base + static_cast<long long>(zg) * np * nq;
-    for (int p = p_lo; p <= p_hi; ++p) {
-        const double qs = fma(static_cast<double>(p), dq, q0);
-        const double qf = floor(qs);
-        const int qi = static_cast<int>(qf);
-        const float d0 = static_cast<float>(qs - qf);  // in [0, 1)
-        const float4* row = plane + static_cast<long long>(p) * nq;
-#pragma unroll
-        for (int k = -1; k <= 2; ++k) {
-            const int q = qi + k;
-            const float tt = (static_cast<float>(k) - d0) * kqf;  // s - b for pixel q
-            float wgt = 1.0f - fabsf(tt);
-            if (first && tt < 0.0f) wgt = 0.0f;
-            if (last && tt >= 0.0f && tt < 1.0f) wgt = 1.0f;
-            if (wgt > 0.0f && q >= 0 && q < nq) {
-                const float4 v = __ldg(row + q);
-                acc.x = fmaf(wgt, v.x, acc.x);
-                acc.y = fmaf(wgt, v.y, acc.y);
-                acc.z = fmaf(wgt, v.z, acc.z);
-                acc.w = fmaf(wgt, v.w, acc.w);
+    if (p_hi < p_lo) {
+        // no ray of this CTA meets the image
+        if (b < nd)
+            for (int j = 0; j < 8; ++j) {
+                const int z = 4 * g0 + j;
+                if (z < nz) sino[(static_cast<long long>(z) * na + a) * nd + b] = 0.0f;
+            }
+        return;
+    }
+    const int nch = (p_hi - p_lo + PCH) / PCH;
+
+    if (t == 0) {
+        for (int i = 0; i < FNB; ++i) mbar_init(&bar[i], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    const long long plane_sz = static_cast<long long>(np) * nq;
+    const float4* plane0 = base + static_cast<long long>(g0) * plane_sz;
+    const float4* plane1 = plane0 + plane_sz;
+
+    // first staged pixel of chunk `ci` (block-uniform, double precision)
+    auto chunk_qs = [&](int ci) -> int {
+        const double p0 = p_lo + ci * PCH;
+        const double e0 = qb0 + p0 * dq, e1 = qb1 + p0 * dq;
+        const double e2 = e0 + (PCH - 1) * dq, e3 = e1 + (PCH - 1) * dq;
+        return static_cast<int>(floor(fmin(fmin(e0, e1), fmin(e2, e3)))) - 3;
+    };
+
+    auto issue = [&](int ci, int buf) {
+        const int p0 = p_lo + ci * PCH;
+        const int qs = chunk_qs(ci);
+        const int lo = max(qs, 0), hi = min(qs + FW - 1, nq - 1);  // in-image part
+        const int npl = has_g1 ? 2 : 1;
+        // zero the staged pixels that lie outside the image (or beyond the last row / plane)
+        for (int i = t; i < 2 * PCH * FW; i += FB) {
+            const int pl = i / (PCH * FW), pp = (i / FW) % PCH, q = qs + i % FW;
+            const bool live = pl < npl && p0 + pp < np && q >= lo && q <= hi;
+            if (!live) seg[((buf * 2 + pl) * PCH + pp) * FW + (i % FW)] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        // order these generic-proxy stores before later bulk copies into the buffer
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const unsigned row_bytes = hi >= lo ? static_cast<unsigned>((hi - lo + 1) * sizeof(float4)) : 0u;
+        if (t < 2 * PCH) {
+            const int pl = t / PCH, pp = t % PCH;
+            if (row_bytes && pl < npl && p0 + pp < np) {
+                const float4* src = (pl ? plane1 : plane0) + static_cast<long long>(p0 + pp) * nq + lo;
+                bulk_load(&seg[((buf * 2 + pl) * PCH + pp) * FW + (lo - qs)], src, row_bytes, &bar[buf]);
             }
         }
-    }
-    const float r[4] = {acc.x, acc.y, acc.z, acc.w};
+        if (t == 0) {
+            const int rows_live = max(0, min(PCH, np - p0));
+            mbar_expect_tx(&bar[buf], row_bytes * rows_live * npl);
+        }
+    };
+
+    const float R = static_cast<float>(fabs(inv));
+    const float kqf = static_cast<float>(kq);
+    const float dqf = static_cast<float>(dq);
+    const bool live = b < nd;
+    const bool edge = live && (b == 0 || b == nd - 1);
+    // the reference's float projection for the edge rays
+    const float2 tf = trig.csf[a];
+    const float cxf = static_cast<float>(w - 1) * 0.5f, cyf = static_cast<float>(h - 1) * 0.5f;
+    const float dcs = static_cast<float>(nd / 2);
+
+    float4 acc0 = make_float4(0.f, 0.f, 0.f, 0.f), acc1 = acc0;
+    issue(0, 0);
+    __syncthreads();
+    bool ok_all = true;
+    for (int ci = 0; ci < nch; ++ci) {
+        const int buf = ci & 1;
+        if (ci + 1 < nch) issue(ci + 1, (ci + 1) & 1);
+        const bool landed = mbar_wait_bounded(&bar[buf], (ci >> 1) & 1, err);
+        const int p0 = p_lo + ci * PCH;
+        const int qs = chunk_qs(ci);
+        // crossing point of this ray at p0, relative to the staged segment
+        const double qstar = fma(static_cast<double>(p0), dq, q0);
+        const double qfl = floor(qstar);
+        const float lq0 = static_cast<float>(static_cast<int>(qfl) - qs) + static_cast<float>(qstar - qfl);
+        const float4* s0 = seg + (buf * 2 + 0) * PCH * FW;
+        const float4* s1 = seg + (buf * 2 + 1) * PCH * FW;
+        if (live) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int z = 4 * zg + j;
+            for (int pp = 0; pp < PCH; ++pp) {
+                const float qf = fmaf(static_cast<float>(pp), dqf, lq0);
+                const float qa = ceilf(qf - R);
+                const int ia = static_cast<int>(qa);
+                const float t0 = (qa - qf) * kqf;  // s - b at candidate qa
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float tt = fmaf(static_cast<float>(k), kqf, t0);
+                    float wgt = fmaxf(0.0f, 1.0f - fabsf(tt));
+                    if (edge) {
+                        // SerialBackend.cpp:109-120 on the reference's float s
+                        const int qg = qs + ia + k;
+                        const int pg = p0 + pp;
+                        const float xg = static_cast<float>(rows ? qg : pg);
+                        const float yg = static_cast<float>(rows ? pg : qg);
+                        const float ss = __fadd_rn(__fadd_rn(__fmul_rn(__fsub_rn(xg, cxf), tf.x),
+                                                             __fmul_rn(__fsub_rn(yg, cyf), tf.y)), dcs);
+                        const int i0 = static_cast<int>(floorf(ss));
+                        wgt = 0.0f;
+                        if (i0 >= 0 && i0 < nd - 1) {
+                            if (i0 == b) wgt = 1.0f - tt;
+                            else if (i0 + 1 == b) wgt = 1.0f + tt;
+                        } else if (i0 == nd - 1 && b == nd - 1) {
+                            wgt = 1.0f;
+                        }
+                        wgt = fminf(fmaxf(wgt, 0.0f), 1.0f);
+                    }
+                    const int idx = pp * FW + ia + k;
+                    const float4 v0 = s0[idx], v1 = s1[idx];
+                    acc0.x = fmaf(wgt, v0.x, acc0.x);
+                    acc0.y = fmaf(wgt, v0.y, acc0.y);
+                    acc0.z = fmaf(wgt, v0.z, acc0.z);
+                    acc0.w = fmaf(wgt, v0.w, acc0.w);
+                    acc1.x = fmaf(wgt, v1.x, acc1.x);
+                    acc1.y = fmaf(wgt, v1.y, acc1.y);
+                    acc1.z = fmaf(wgt, v1.z, acc1.z);
+                    acc1.w = fmaf(wgt, v1.w, acc1.w);
+                }
+            }
+        }
+        if (!__syncthreads_and(landed)) { ok_all = false; break; }
+    }
+    if (!ok_all || !live) return;
+    const float r[8] = {acc0.x, acc0.y, acc0.z, acc0.w, acc1.x, acc1.y, acc1.z, acc1.w};
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int z = 4 * g0 + j;
         if (z < nz) sino[(static_cast<long long>(z) * na + a) * nd + b] = r[j];
     }
 }
@@ -216,9 +382,15 @@ cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const flo
 }
 
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
-                           int na, int nd, const double2* d_cs, float* d_sino, cudaStream_t st) {
-    const dim3 grid((nd + 127) / 128, na, (nz + 3) / 4);
-    k_forward<<<grid, 128, 0, st>>>(d_img, d_imgT, w, h, nz, na, nd, d_cs, d_sino);
+                           int na, int nd, Trig trig, float* d_sino, unsigned* d_err,
+                           cudaStream_t st) {
+    const size_t smem = sizeof(float4) * FNB * 2 * PCH * FW + sizeof(unsigned long long) * FNB;
+    const cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const int nzg = (nz + 3) / 4;
+    const dim3 grid((nd + FB - 1) / FB, na, (nzg + 1) / 2);
+    k_forward<<<grid, FB, smem, st>>>(d_img, d_imgT, w, h, nz, na, nd, trig, d_sino, d_err);
     return cudaGetLastError();
 }
 
