@@ -147,6 +147,7 @@ ctb_status trig_table(ctb_ctx* ctx, const float* angles_deg, int na, Trig* out) 
             ctx->user_angles.clear();
             CTB_TRY(fill_trig(ctx, angles_deg, na, table));
             ctx->user_angles.assign(angles_deg, angles_deg + na);
+            ++ctx->user_angles_gen;
         }
     }
     out->cs = static_cast<const double2*>(table);
@@ -215,6 +216,33 @@ void mark(ctb_ctx* ctx, cudaEvent_t* ev, int k) {
     if (ev) cudaEventRecord(ev[k], ctx->stream);
 }
 
+// Angle groups of the forward projector for this geometry (cached; explicit
+// angle lists are keyed by their upload generation).
+ctb_status forward_plan_dev(ctb_ctx* ctx, const float* angles_deg, int na, int w, int h, int nd,
+                            const ctb_ctx::FwdPlanDev** out) {
+    const std::vector<long long> key = {angles_deg ? ctx->user_angles_gen : -1, na, w, h, nd};
+    auto it = ctx->fwd_plans.find(key);
+    if (it == ctx->fwd_plans.end()) {
+        std::vector<float> uni;
+        if (!angles_deg) {
+            uni = uniform_angles(na);
+            angles_deg = uni.data();
+        }
+        const FwdPlan plan = forward_plan(angles_deg, na, w, h, nd);
+        ctb_ctx::FwdPlanDev d;
+        d.ngroups = static_cast<int>(plan.groups.size() / 4);
+        CTB_CUDA(ctx, cudaMalloc(&d.groups.ptr, sizeof(int) * plan.groups.size()));
+        CTB_CUDA(ctx, cudaMalloc(&d.order.ptr, sizeof(int) * plan.order.size()));
+        CTB_CUDA(ctx, cudaMemcpy(d.groups.ptr, plan.groups.data(), sizeof(int) * plan.groups.size(),
+                                 cudaMemcpyHostToDevice));
+        CTB_CUDA(ctx, cudaMemcpy(d.order.ptr, plan.order.data(), sizeof(int) * plan.order.size(),
+                                 cudaMemcpyHostToDevice));
+        it = ctx->fwd_plans.emplace(key, d).first;
+    }
+    *out = &it->second;
+    return CTB_OK;
+}
+
 ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz, int na, int nd,
                          const float* angles_deg, float* d_sino, float4* d_stats,
                          cudaEvent_t* ev = nullptr) {
@@ -227,7 +255,11 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream));
     CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream));
     mark(ctx, ev, 1);
-    CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd, trig, d_sino, ctx->d_err,
+    const ctb_ctx::FwdPlanDev* plan = nullptr;
+    CTB_TRY(forward_plan_dev(ctx, angles_deg, na, w, h, nd, &plan));
+    CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd, trig,
+                                   static_cast<const int4*>(plan->groups.ptr), plan->ngroups,
+                                   static_cast<const int*>(plan->order.ptr), d_sino, ctx->d_err,
                                    ctx->stream));
     return CTB_OK;
 }
@@ -320,6 +352,10 @@ void ctb_destroy(ctb_ctx* ctx) {
         for (auto& kv : ctx->filters) cudaFree(kv.second.ptr);
         for (auto& kv : ctx->twiddles) cudaFree(kv.second.ptr);
         for (auto& kv : ctx->trig_uniform) cudaFree(kv.second.ptr);
+        for (auto& kv : ctx->fwd_plans) {
+            cudaFree(kv.second.groups.ptr);
+            cudaFree(kv.second.order.ptr);
+        }
         for (auto& e : ctx->prof_ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : ctx->ev)

@@ -63,9 +63,22 @@ cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4
                                cudaStream_t st);
 cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
                              float4* d_img, float4* d_imgT, cudaStream_t st);
+// Forward projector work plan: angles grouped (up to kFwdGroup per CTA) by
+// walked axis so that one staged row segment of kFwdWidth pixels serves every
+// angle of the group. groups: {first index into order, count, axis (0 rows,
+// 1 columns), 0}.
+constexpr int kFwdRays = 128;   // rays (detector bins) per CTA
+constexpr int kFwdRows = 8;     // walked rows per staged chunk
+constexpr int kFwdWidth = 256;  // staged pixels per row
+constexpr int kFwdGroup = 8;    // angles per CTA
+struct FwdPlan {
+    std::vector<int> order;
+    std::vector<int> groups;  // 4 ints per group
+};
+FwdPlan forward_plan(const float* angles_deg, int na, int w, int h, int nd);
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
-                           int na, int nd, Trig trig, float* d_sino, unsigned* d_err,
-                           cudaStream_t st);
+                           int na, int nd, Trig trig, const int4* d_groups, int ngroups,
+                           const int* d_order, float* d_sino, unsigned* d_err, cudaStream_t st);
 cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
                           const FiltLayout& fl, const float* d_Hs, const float2* d_tw,
                           const float4* d_stats, int denorm, float scale, float4* d_filt,
@@ -105,6 +118,13 @@ struct ctb_ctx {
     // Angle tables: uniform angle sets per count; the last explicit list.
     std::map<int, ctb::DevBuf> trig_uniform;
     std::vector<float> user_angles;
+    long long user_angles_gen = 0;  // bumps whenever the explicit angle list changes
+    // Forward projector plans (angle groups) per (angle set, w, h, nd).
+    struct FwdPlanDev {
+        ctb::DevBuf groups, order;
+        int ngroups = 0;
+    };
+    std::map<std::vector<long long>, FwdPlanDev> fwd_plans;
     unsigned* d_err = nullptr;  // device error word for bounded waits
 
     // Stage profiling: a ring of event sets, one set per volume reconstruction.

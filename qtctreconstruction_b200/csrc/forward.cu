@@ -120,23 +120,28 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
 }
 
 // ----------------------------------------------------------------- forward
-// A CTA owns FB = 128 consecutive detector bins (rays) of one angle and eight
-// slices (two float4 planes of the normalised image). The ray family is walked
-// along the image axis it is closest to (rows when |cos| >= |sin|, else
-// columns of the transposed copy), so every step crosses at most three pixels
-// of the gathered axis. Rows are processed in chunks of PCH = 8; per chunk the
-// row segments the CTA's rays can touch (FW pixels per row and plane) are
-// staged into shared memory by the bulk-copy engine, double-buffered on
-// mbarriers, with zeros where a segment leaves the image. The crossing point
-// q*(b, p) is evaluated in double once per chunk and split into an integer
-// and a float fraction; within the chunk each thread steps in float on small
-// numbers. The two edge rays (bins 0 and nd-1), where the reference's rules
-// are discontinuous, decide which pixels count with the reference's own float
+// A CTA owns FB = 128 consecutive detector bins (rays), one group of up to
+// GMAX = 8 angles that share the walked image axis, and four slices (one
+// float4 plane of the normalised image). The ray family is walked along the
+// image axis it is closest to (rows when |cos| >= |sin|, else columns of the
+// transposed copy), so every step crosses at most three pixels of the
+// gathered axis. Rows are processed in chunks of PCH = 8; per chunk the row
+// segments the CTA's rays of all its angles can touch (FW pixels per row) are
+// staged once into shared memory by the bulk-copy engine, double-buffered on
+// mbarriers, with zeros where a segment leaves the image, and reused by every
+// angle of the group. The host forms the groups so that the segment width
+// provably fits (forward_plan). The crossing point q*(b, p) is evaluated in
+// double once per chunk and angle and split into an integer and a float
+// fraction; within the chunk each thread steps in float on small numbers. The
+// two edge rays (bins 0 and nd-1), where the reference's rules are
+// discontinuous, decide which pixels count with the reference's own float
 // arithmetic (SerialBackend.cpp:109-120).
-constexpr int FB = 128;   // rays per CTA
-constexpr int PCH = 8;    // walked rows per chunk
-constexpr int FW = 200;   // staged pixels per row and plane (>= 127 sqrt(2) + 7 + 8)
-constexpr int FNB = 2;    // chunk buffers
+constexpr int FB = kFwdRays;
+constexpr int PCH = kFwdRows;
+constexpr int FW = kFwdWidth;
+constexpr int GMAX = kFwdGroup;
+constexpr int FNB = 2;           // chunk buffers
+constexpr int MAXCH = 512;       // chunk table capacity (np <= 4096)
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -177,122 +182,149 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     return false;
 }
 
+struct FAngle {
+    double q0b0;  // q*(b0, p = 0)
+    double inv;   // dq*/db = 1 / kq
+    double dq;    // dq*/dp = -kp / kq
+    float kqf, R, dqf;
+    float cf, sf;  // the reference's float cos/sin
+    int a;
+    int p_lo, p_hi;
+};
+
 __global__ void __launch_bounds__(FB) k_forward(const float4* __restrict__ img,
                                                 const float4* __restrict__ imgT, int w, int h,
                                                 int nz, int na, int nd, Trig trig,
+                                                const int4* __restrict__ groups,
+                                                const int* __restrict__ order,
                                                 float* __restrict__ sino, unsigned* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    float4* seg = reinterpret_cast<float4*>(smem_raw);  // [FNB][2][PCH][FW]
-    auto bar = reinterpret_cast<unsigned long long*>(smem_raw + sizeof(float4) * FNB * 2 * PCH * FW);
+    float4* seg = reinterpret_cast<float4*>(smem_raw);  // [FNB][PCH][FW]
+    unsigned char* tail = smem_raw + sizeof(float4) * FNB * PCH * FW;
+    auto bar = reinterpret_cast<unsigned long long*>(tail);
+    auto fa = reinterpret_cast<FAngle*>(tail + 16);
+    auto qs_tab = reinterpret_cast<int*>(tail + 16 + sizeof(FAngle) * GMAX);
 
-    const int a = blockIdx.y;
     const int b0 = blockIdx.x * FB;
     const int b1 = min(b0 + FB, nd);  // exclusive
-    const int nzg = (nz + 3) / 4;
-    const int g0 = 2 * blockIdx.z;
-    const bool has_g1 = g0 + 1 < nzg;
+    const int4 grp = groups[blockIdx.y];
+    const int cnt = grp.y;
+    const bool rows = grp.z == 0;
+    const int g = blockIdx.z;  // slice group (4 slices)
     const int t = threadIdx.x;
     const int b = b0 + t;
 
-    const double2 tc = trig.cs[a];
-    const double c = tc.x, s = tc.y;
-    const bool rows = fabs(c) >= fabs(s);
-    const float4* base = rows ? img : imgT;
     const int np = rows ? h : w;  // walked axis
     const int nq = rows ? w : h;  // gathered axis
-    const double kq = rows ? c : s;
-    const double kp = rows ? s : c;
     const double cq = rows ? 0.5 * (w - 1) : 0.5 * (h - 1);
     const double cp = rows ? 0.5 * (h - 1) : 0.5 * (w - 1);
     const double dcf = static_cast<double>(nd / 2);
-    // s(q, p) = (q - cq) kq + (p - cp) kp + dcf = b  <=>  q = q0(b) + p dq
-    const double inv = 1.0 / kq;
-    const double dq = -kp * inv;
-    const double qb0 = cq + (static_cast<double>(b0) - dcf + cp * kp) * inv;
-    const double qb1 = cq + (static_cast<double>(b1 - 1) - dcf + cp * kp) * inv;
-    const double q0 = cq + (static_cast<double>(b) - dcf + cp * kp) * inv;
-    const double reach = fabs(inv) + 2.0;
 
-    // walked range touched by any of the CTA's rays (block-uniform)
-    int p_lo = 0, p_hi = np - 1;
-    if (dq != 0.0) {
-        double pa0 = (-reach - qb0) / dq, pb0 = (nq - 1 + reach - qb0) / dq;
-        double pa1 = (-reach - qb1) / dq, pb1 = (nq - 1 + reach - qb1) / dq;
-        const double lo = fmin(fmin(pa0, pb0), fmin(pa1, pb1));
-        const double hi = fmax(fmax(pa0, pb0), fmax(pa1, pb1));
-        p_lo = max(0, static_cast<int>(floor(lo)) - 1);
-        p_hi = min(np - 1, static_cast<int>(ceil(hi)) + 1);
-    } else {
-        const double qlo = fmin(qb0, qb1), qhi = fmax(qb0, qb1);
-        if (qhi < -reach || qlo > nq - 1 + reach) p_hi = -1;
+    if (t < cnt) {
+        const int a = order[grp.x + t];
+        const double2 tc = trig.cs[a];
+        const double kq = rows ? tc.x : tc.y;
+        const double kp = rows ? tc.y : tc.x;
+        // s(q, p) = (q - cq) kq + (p - cp) kp + dcf = b  <=>  q = q0(b) + p dq
+        FAngle f;
+        f.inv = 1.0 / kq;
+        f.dq = -kp * f.inv;
+        f.q0b0 = cq + (static_cast<double>(b0) - dcf + cp * kp) * f.inv;
+        f.kqf = static_cast<float>(kq);
+        f.R = static_cast<float>(fabs(f.inv));
+        f.dqf = static_cast<float>(f.dq);
+        const float2 tf = trig.csf[a];
+        f.cf = tf.x;
+        f.sf = tf.y;
+        f.a = a;
+        // walked range whose crossings lie within reach of the image, over the CTA's rays
+        const double reach = fabs(f.inv) + 2.0;
+        const double qb1 = f.q0b0 + (b1 - 1 - b0) * f.inv;
+        int lo = 0, hi = np - 1;
+        if (f.dq != 0.0) {
+            const double pa0 = (-reach - f.q0b0) / f.dq, pb0 = (nq - 1 + reach - f.q0b0) / f.dq;
+            const double pa1 = (-reach - qb1) / f.dq, pb1 = (nq - 1 + reach - qb1) / f.dq;
+            lo = max(0, static_cast<int>(floor(fmin(fmin(pa0, pb0), fmin(pa1, pb1)))) - 1);
+            hi = min(np - 1, static_cast<int>(ceil(fmax(fmax(pa0, pb0), fmax(pa1, pb1)))) + 1);
+        } else if (fmax(f.q0b0, qb1) < -reach || fmin(f.q0b0, qb1) > nq - 1 + reach) {
+            hi = -1;
+        }
+        f.p_lo = lo;
+        f.p_hi = hi;
+        fa[t] = f;
     }
-    if (p_hi < p_lo) {
-        // no ray of this CTA meets the image
-        if (b < nd)
-            for (int j = 0; j < 8; ++j) {
-                const int z = 4 * g0 + j;
-                if (z < nz) sino[(static_cast<long long>(z) * na + a) * nd + b] = 0.0f;
-            }
-        return;
-    }
-    const int nch = (p_hi - p_lo + PCH) / PCH;
-
     if (t == 0) {
         for (int i = 0; i < FNB; ++i) mbar_init(&bar[i], 1);
         mbar_fence_init();
     }
     __syncthreads();
-
+    int p_lo = np, p_hi = -1;
+    for (int j = 0; j < cnt; ++j) {
+        if (fa[j].p_hi >= fa[j].p_lo) {
+            p_lo = min(p_lo, fa[j].p_lo);
+            p_hi = max(p_hi, fa[j].p_hi);
+        }
+    }
     const long long plane_sz = static_cast<long long>(np) * nq;
-    const float4* plane0 = base + static_cast<long long>(g0) * plane_sz;
-    const float4* plane1 = plane0 + plane_sz;
-
-    // first staged pixel of chunk `ci` (block-uniform, double precision)
-    auto chunk_qs = [&](int ci) -> int {
+    const bool live = b < nd;
+    if (p_hi < p_lo) {  // no ray of this CTA meets the image
+        if (live)
+            for (int j = 0; j < cnt; ++j)
+                for (int k = 0; k < 4; ++k) {
+                    const int z = 4 * g + k;
+                    if (z < nz) sino[(static_cast<long long>(z) * na + fa[j].a) * nd + b] = 0.0f;
+                }
+        return;
+    }
+    const int nch = (p_hi - p_lo + PCH) / PCH;
+    // first staged pixel of every chunk: minimum crossing over angles and corners
+    for (int ci = t; ci < nch; ci += FB) {
         const double p0 = p_lo + ci * PCH;
-        const double e0 = qb0 + p0 * dq, e1 = qb1 + p0 * dq;
-        const double e2 = e0 + (PCH - 1) * dq, e3 = e1 + (PCH - 1) * dq;
-        return static_cast<int>(floor(fmin(fmin(e0, e1), fmin(e2, e3)))) - 3;
-    };
+        double m = 1e300;
+        for (int j = 0; j < cnt; ++j) {
+            const double qa0 = fma(p0, fa[j].dq, fa[j].q0b0);
+            const double qa1 = qa0 + (b1 - 1 - b0) * fa[j].inv;
+            const double e = (PCH - 1) * fa[j].dq;
+            m = fmin(m, fmin(fmin(qa0, qa1), fmin(qa0 + e, qa1 + e)));
+        }
+        qs_tab[ci] = static_cast<int>(floor(m)) - 3;
+    }
+    __syncthreads();
+
+    const float4* plane = (rows ? img : imgT) + static_cast<long long>(g) * plane_sz;
 
     auto issue = [&](int ci, int buf) {
         const int p0 = p_lo + ci * PCH;
-        const int qs = chunk_qs(ci);
+        const int qs = qs_tab[ci];
         const int lo = max(qs, 0), hi = min(qs + FW - 1, nq - 1);  // in-image part
-        const int npl = has_g1 ? 2 : 1;
-        // zero the staged pixels that lie outside the image (or beyond the last row / plane)
-        for (int i = t; i < 2 * PCH * FW; i += FB) {
-            const int pl = i / (PCH * FW), pp = (i / FW) % PCH, q = qs + i % FW;
-            const bool live = pl < npl && p0 + pp < np && q >= lo && q <= hi;
-            if (!live) seg[((buf * 2 + pl) * PCH + pp) * FW + (i % FW)] = make_float4(0.f, 0.f, 0.f, 0.f);
+        const bool any = hi >= lo;
+        // zero the staged pixels outside the image and whole rows beyond the last one
+        {
+            const int pp = t >> 4, sub = t & 15;
+            float4* row = seg + (buf * PCH + pp) * FW;
+            const bool dead = !any || p0 + pp >= np;
+            const int pre = dead ? FW : lo - qs, post = dead ? FW : hi - qs + 1;
+            for (int i = sub; i < pre; i += 16) row[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int i = post + sub; i < FW; i += 16) row[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        // order these generic-proxy stores before later bulk copies into the buffer
+        // order the generic-proxy stores before later bulk copies into this buffer
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        const unsigned row_bytes = hi >= lo ? static_cast<unsigned>((hi - lo + 1) * sizeof(float4)) : 0u;
-        if (t < 2 * PCH) {
-            const int pl = t / PCH, pp = t % PCH;
-            if (row_bytes && pl < npl && p0 + pp < np) {
-                const float4* src = (pl ? plane1 : plane0) + static_cast<long long>(p0 + pp) * nq + lo;
-                bulk_load(&seg[((buf * 2 + pl) * PCH + pp) * FW + (lo - qs)], src, row_bytes, &bar[buf]);
-            }
-        }
-        if (t == 0) {
-            const int rows_live = max(0, min(PCH, np - p0));
-            mbar_expect_tx(&bar[buf], row_bytes * rows_live * npl);
-        }
+        const unsigned row_bytes = any ? static_cast<unsigned>((hi - lo + 1) * sizeof(float4)) : 0u;
+        if (t < PCH && row_bytes && p0 + t < np)
+            bulk_load(seg + (buf * PCH + t) * FW + (lo - qs), plane + static_cast<long long>(p0 + t) * nq + lo,
+                      row_bytes, &bar[buf]);
+        if (t == 0) mbar_expect_tx(&bar[buf], row_bytes * max(0, min(PCH, np - p0)));
     };
 
-    const float R = static_cast<float>(fabs(inv));
-    const float kqf = static_cast<float>(kq);
-    const float dqf = static_cast<float>(dq);
-    const bool live = b < nd;
-    const bool edge = live && (b == 0 || b == nd - 1);
     // the reference's float projection for the edge rays
-    const float2 tf = trig.csf[a];
+    const bool edge = live && (b == 0 || b == nd - 1);
     const float cxf = static_cast<float>(w - 1) * 0.5f, cyf = static_cast<float>(h - 1) * 0.5f;
     const float dcs = static_cast<float>(nd / 2);
 
-    float4 acc0 = make_float4(0.f, 0.f, 0.f, 0.f), acc1 = acc0;
+    float4 acc[GMAX];
+#pragma unroll
+    for (int j = 0; j < GMAX; ++j) acc[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+
     issue(0, 0);
     __syncthreads();
     bool ok_all = true;
@@ -301,63 +333,67 @@ __global__ void __launch_bounds__(FB) k_forward(const float4* __restrict__ img,
         if (ci + 1 < nch) issue(ci + 1, (ci + 1) & 1);
         const bool landed = mbar_wait_bounded(&bar[buf], (ci >> 1) & 1, err);
         const int p0 = p_lo + ci * PCH;
-        const int qs = chunk_qs(ci);
-        // crossing point of this ray at p0, relative to the staged segment
-        const double qstar = fma(static_cast<double>(p0), dq, q0);
-        const double qfl = floor(qstar);
-        const float lq0 = static_cast<float>(static_cast<int>(qfl) - qs) + static_cast<float>(qstar - qfl);
-        const float4* s0 = seg + (buf * 2 + 0) * PCH * FW;
-        const float4* s1 = seg + (buf * 2 + 1) * PCH * FW;
+        const int qs = qs_tab[ci];
+        const float4* sg = seg + buf * PCH * FW;
         if (live) {
 #pragma unroll
-            for (int pp = 0; pp < PCH; ++pp) {
-                const float qf = fmaf(static_cast<float>(pp), dqf, lq0);
-                const float qa = ceilf(qf - R);
-                const int ia = static_cast<int>(qa);
-                const float t0 = (qa - qf) * kqf;  // s - b at candidate qa
+            for (int j = 0; j < GMAX; ++j) {
+                if (j >= cnt) break;
+                const FAngle f = fa[j];
+                // crossing of this ray at p0, relative to the staged segment
+                const double qstar = fma(static_cast<double>(p0), f.dq, fma(static_cast<double>(t), f.inv, f.q0b0));
+                const double qfl = floor(qstar);
+                const float lq0 = static_cast<float>(static_cast<int>(qfl) - qs) + static_cast<float>(qstar - qfl);
 #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const float tt = fmaf(static_cast<float>(k), kqf, t0);
-                    float wgt = fmaxf(0.0f, 1.0f - fabsf(tt));
-                    if (edge) {
-                        // SerialBackend.cpp:109-120 on the reference's float s
-                        const int qg = qs + ia + k;
-                        const int pg = p0 + pp;
-                        const float xg = static_cast<float>(rows ? qg : pg);
-                        const float yg = static_cast<float>(rows ? pg : qg);
-                        const float ss = __fadd_rn(__fadd_rn(__fmul_rn(__fsub_rn(xg, cxf), tf.x),
-                                                             __fmul_rn(__fsub_rn(yg, cyf), tf.y)), dcs);
-                        const int i0 = static_cast<int>(floorf(ss));
-                        wgt = 0.0f;
-                        if (i0 >= 0 && i0 < nd - 1) {
-                            if (i0 == b) wgt = 1.0f - tt;
-                            else if (i0 + 1 == b) wgt = 1.0f + tt;
-                        } else if (i0 == nd - 1 && b == nd - 1) {
-                            wgt = 1.0f;
+                for (int pp = 0; pp < PCH; ++pp) {
+                    const float qf = fmaf(static_cast<float>(pp), f.dqf, lq0);
+                    const float qa = ceilf(qf - f.R);
+                    const int ia = static_cast<int>(qa);
+                    const float t0 = (qa - qf) * f.kqf;  // s - b at candidate qa
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const float tt = fmaf(static_cast<float>(k), f.kqf, t0);
+                        float wgt = fmaxf(0.0f, 1.0f - fabsf(tt));
+                        if (edge) {
+                            // SerialBackend.cpp:109-120 on the reference's float s
+                            const int qg = qs + ia + k;
+                            const int pg = p0 + pp;
+                            const float xg = static_cast<float>(rows ? qg : pg);
+                            const float yg = static_cast<float>(rows ? pg : qg);
+                            const float ss = __fadd_rn(__fadd_rn(__fmul_rn(__fsub_rn(xg, cxf), f.cf),
+                                                                 __fmul_rn(__fsub_rn(yg, cyf), f.sf)), dcs);
+                            const int i0 = static_cast<int>(floorf(ss));
+                            wgt = 0.0f;
+                            if (i0 >= 0 && i0 < nd - 1) {
+                                if (i0 == b) wgt = 1.0f - tt;
+                                else if (i0 + 1 == b) wgt = 1.0f + tt;
+                            } else if (i0 == nd - 1 && b == nd - 1) {
+                                wgt = 1.0f;
+                            }
+                            wgt = fminf(fmaxf(wgt, 0.0f), 1.0f);
                         }
-                        wgt = fminf(fmaxf(wgt, 0.0f), 1.0f);
+                        const float4 v = sg[pp * FW + ia + k];
+                        acc[j].x = fmaf(wgt, v.x, acc[j].x);
+                        acc[j].y = fmaf(wgt, v.y, acc[j].y);
+                        acc[j].z = fmaf(wgt, v.z, acc[j].z);
+                        acc[j].w = fmaf(wgt, v.w, acc[j].w);
                     }
-                    const int idx = pp * FW + ia + k;
-                    const float4 v0 = s0[idx], v1 = s1[idx];
-                    acc0.x = fmaf(wgt, v0.x, acc0.x);
-                    acc0.y = fmaf(wgt, v0.y, acc0.y);
-                    acc0.z = fmaf(wgt, v0.z, acc0.z);
-                    acc0.w = fmaf(wgt, v0.w, acc0.w);
-                    acc1.x = fmaf(wgt, v1.x, acc1.x);
-                    acc1.y = fmaf(wgt, v1.y, acc1.y);
-                    acc1.z = fmaf(wgt, v1.z, acc1.z);
-                    acc1.w = fmaf(wgt, v1.w, acc1.w);
                 }
             }
         }
         if (!__syncthreads_and(landed)) { ok_all = false; break; }
     }
     if (!ok_all || !live) return;
-    const float r[8] = {acc0.x, acc0.y, acc0.z, acc0.w, acc1.x, acc1.y, acc1.z, acc1.w};
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const int z = 4 * g0 + j;
-        if (z < nz) sino[(static_cast<long long>(z) * na + a) * nd + b] = r[j];
+    for (int j = 0; j < GMAX; ++j) {
+        if (j >= cnt) break;
+        const float r[4] = {acc[j].x, acc[j].y, acc[j].z, acc[j].w};
+        const long long a = fa[j].a;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int z = 4 * g + k;
+            if (z < nz) sino[(static_cast<long long>(z) * na + a) * nd + b] = r[k];
+        }
     }
 }
 
@@ -382,15 +418,18 @@ cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const flo
 }
 
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
-                           int na, int nd, Trig trig, float* d_sino, unsigned* d_err,
-                           cudaStream_t st) {
-    const size_t smem = sizeof(float4) * FNB * 2 * PCH * FW + sizeof(unsigned long long) * FNB;
+                           int na, int nd, Trig trig, const int4* d_groups, int ngroups,
+                           const int* d_order, float* d_sino, unsigned* d_err, cudaStream_t st) {
+    const size_t smem = sizeof(float4) * FNB * PCH * FW + 16 + sizeof(FAngle) * GMAX +
+                        sizeof(int) * MAXCH;
     const cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    const int nzg = (nz + 3) / 4;
-    const dim3 grid((nd + FB - 1) / FB, na, (nzg + 1) / 2);
-    k_forward<<<grid, FB, smem, st>>>(d_img, d_imgT, w, h, nz, na, nd, trig, d_sino, d_err);
+    const int np = w > h ? w : h;
+    if ((np + PCH - 1) / PCH + 1 > MAXCH) return cudaErrorInvalidValue;
+    const dim3 grid((nd + FB - 1) / FB, ngroups, (nz + 3) / 4);
+    k_forward<<<grid, FB, smem, st>>>(d_img, d_imgT, w, h, nz, na, nd, trig, d_groups, d_order,
+                                      d_sino, d_err);
     return cudaGetLastError();
 }
 
