@@ -1,16 +1,6 @@
-// forward.cu — angle tables, per-slice statistics, normalisation and the
-// ray-driven forward projector (RadonTransform stage of the FBP path).
-//
-// The reference's forward projector (SerialBackend::computeSinogram,
-// SerialBackend.cpp:59-136) splats every non-zero pixel onto the two detector
-// bins around s = (x-cx)cos + (y-cy)sin + floor(nd/2) with linear weights.
-// Here the same linear operator is evaluated as a gather: each thread owns one
-// detector bin (a ray) of one angle for four slices and walks the ray through
-// the image, collecting the pixels whose splat reaches its bin with the tent
-// weight 1 - |s - b| (the identical weights (1-frac, frac) of the splat). The
-// reference's edge rules are kept: bin 0 takes nothing from pixels with s < 0
-// and bin nd-1 takes the full value from pixels with s in [nd-1, nd).
-// Sinogram stores are coalesced by detector bin.
+// forward.cu — preparation kernels of the forward projection: angle tables,
+// per-slice statistics and the normalised, slice-interleaved image copies the
+// projector reads (forward_proj.cu holds the projector itself).
 #include <cfloat>
 #include <cmath>
 
@@ -119,284 +109,6 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
     }
 }
 
-// ----------------------------------------------------------------- forward
-// A CTA owns FB = 128 consecutive detector bins (rays), one group of up to
-// GMAX = 8 angles that share the walked image axis, and four slices (one
-// float4 plane of the normalised image). The ray family is walked along the
-// image axis it is closest to (rows when |cos| >= |sin|, else columns of the
-// transposed copy), so every step crosses at most three pixels of the
-// gathered axis. Rows are processed in chunks of PCH = 8; per chunk the row
-// segments the CTA's rays of all its angles can touch (FW pixels per row) are
-// staged once into shared memory by the bulk-copy engine, double-buffered on
-// mbarriers, with zeros where a segment leaves the image, and reused by every
-// angle of the group. The host forms the groups so that the segment width
-// provably fits (forward_plan). The crossing point q*(b, p) is evaluated in
-// double once per chunk and angle and split into an integer and a float
-// fraction; within the chunk each thread steps in float on small numbers. The
-// two edge rays (bins 0 and nd-1), where the reference's rules are
-// discontinuous, decide which pixels count with the reference's own float
-// arithmetic (SerialBackend.cpp:109-120).
-constexpr int FB = kFwdRays;
-constexpr int PCH = kFwdRows;
-constexpr int FW = kFwdWidth;
-constexpr int GMAX = kFwdGroup;
-constexpr int FNB = 2;           // chunk buffers
-constexpr int MAXCH = 512;       // chunk table capacity (np <= 4096)
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() {
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
-                                          unsigned long long* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
-                                                  unsigned* err) {
-    for (unsigned it = 0; it < (1u << 22); ++it)
-        if (mbar_try_wait(bar, parity)) return true;
-    if (err) atomicOr(err, 2u);
-    return false;
-}
-
-struct FAngle {
-    double q0b0;  // q*(b0, p = 0)
-    double inv;   // dq*/db = 1 / kq
-    double dq;    // dq*/dp = -kp / kq
-    float kqf, R, dqf;
-    float cf, sf;  // the reference's float cos/sin
-    int a;
-    int p_lo, p_hi;
-};
-
-__global__ void __launch_bounds__(FB) k_forward(const float4* __restrict__ img,
-                                                const float4* __restrict__ imgT, int w, int h,
-                                                int nz, int na, int nd, Trig trig,
-                                                const int4* __restrict__ groups,
-                                                const int* __restrict__ order,
-                                                float* __restrict__ sino, unsigned* __restrict__ err) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float4* seg = reinterpret_cast<float4*>(smem_raw);  // [FNB][PCH][FW]
-    unsigned char* tail = smem_raw + sizeof(float4) * FNB * PCH * FW;
-    auto bar = reinterpret_cast<unsigned long long*>(tail);
-    auto fa = reinterpret_cast<FAngle*>(tail + 16);
-    auto qs_tab = reinterpret_cast<int*>(tail + 16 + sizeof(FAngle) * GMAX);
-
-    const int b0 = blockIdx.x * FB;
-    const int b1 = min(b0 + FB, nd);  // exclusive
-    const int4 grp = groups[blockIdx.y];
-    const int cnt = grp.y;
-    const bool rows = grp.z == 0;
-    const int g = blockIdx.z;  // slice group (4 slices)
-    const int t = threadIdx.x;
-    const int b = b0 + t;
-
-    const int np = rows ? h : w;  // walked axis
-    const int nq = rows ? w : h;  // gathered axis
-    const double cq = rows ? 0.5 * (w - 1) : 0.5 * (h - 1);
-    const double cp = rows ? 0.5 * (h - 1) : 0.5 * (w - 1);
-    const double dcf = static_cast<double>(nd / 2);
-
-    if (t < cnt) {
-        const int a = order[grp.x + t];
-        const double2 tc = trig.cs[a];
-        const double kq = rows ? tc.x : tc.y;
-        const double kp = rows ? tc.y : tc.x;
-        // s(q, p) = (q - cq) kq + (p - cp) kp + dcf = b  <=>  q = q0(b) + p dq
-        FAngle f;
-        f.inv = 1.0 / kq;
-        f.dq = -kp * f.inv;
-        f.q0b0 = cq + (static_cast<double>(b0) - dcf + cp * kp) * f.inv;
-        f.kqf = static_cast<float>(kq);
-        f.R = static_cast<float>(fabs(f.inv));
-        f.dqf = static_cast<float>(f.dq);
-        const float2 tf = trig.csf[a];
-        f.cf = tf.x;
-        f.sf = tf.y;
-        f.a = a;
-        // walked range whose crossings lie within reach of the image, over the CTA's rays
-        const double reach = fabs(f.inv) + 2.0;
-        const double qb1 = f.q0b0 + (b1 - 1 - b0) * f.inv;
-        int lo = 0, hi = np - 1;
-        if (f.dq != 0.0) {
-            const double pa0 = (-reach - f.q0b0) / f.dq, pb0 = (nq - 1 + reach - f.q0b0) / f.dq;
-            const double pa1 = (-reach - qb1) / f.dq, pb1 = (nq - 1 + reach - qb1) / f.dq;
-            lo = max(0, static_cast<int>(floor(fmin(fmin(pa0, pb0), fmin(pa1, pb1)))) - 1);
-            hi = min(np - 1, static_cast<int>(ceil(fmax(fmax(pa0, pb0), fmax(pa1, pb1)))) + 1);
-        } else if (fmax(f.q0b0, qb1) < -reach || fmin(f.q0b0, qb1) > nq - 1 + reach) {
-            hi = -1;
-        }
-        f.p_lo = lo;
-        f.p_hi = hi;
-        fa[t] = f;
-    }
-    if (t == 0) {
-        for (int i = 0; i < FNB; ++i) mbar_init(&bar[i], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    int p_lo = np, p_hi = -1;
-    for (int j = 0; j < cnt; ++j) {
-        if (fa[j].p_hi >= fa[j].p_lo) {
-            p_lo = min(p_lo, fa[j].p_lo);
-            p_hi = max(p_hi, fa[j].p_hi);
-        }
-    }
-    const long long plane_sz = static_cast<long long>(np) * nq;
-    const bool live = b < nd;
-    if (p_hi < p_lo) {  // no ray of this CTA meets the image
-        if (live)
-            for (int j = 0; j < cnt; ++j)
-                for (int k = 0; k < 4; ++k) {
-                    const int z = 4 * g + k;
-                    if (z < nz) sino[(static_cast<long long>(z) * na + fa[j].a) * nd + b] = 0.0f;
-                }
-        return;
-    }
-    const int nch = (p_hi - p_lo + PCH) / PCH;
-    // first staged pixel of every chunk: minimum crossing over angles and corners
-    for (int ci = t; ci < nch; ci += FB) {
-        const double p0 = p_lo + ci * PCH;
-        double m = 1e300;
-        for (int j = 0; j < cnt; ++j) {
-            const double qa0 = fma(p0, fa[j].dq, fa[j].q0b0);
-            const double qa1 = qa0 + (b1 - 1 - b0) * fa[j].inv;
-            const double e = (PCH - 1) * fa[j].dq;
-            m = fmin(m, fmin(fmin(qa0, qa1), fmin(qa0 + e, qa1 + e)));
-        }
-        qs_tab[ci] = static_cast<int>(floor(m)) - 3;
-    }
-    __syncthreads();
-
-    const float4* plane = (rows ? img : imgT) + static_cast<long long>(g) * plane_sz;
-
-    auto issue = [&](int ci, int buf) {
-        const int p0 = p_lo + ci * PCH;
-        const int qs = qs_tab[ci];
-        const int lo = max(qs, 0), hi = min(qs + FW - 1, nq - 1);  // in-image part
-        const bool any = hi >= lo;
-        // zero the staged pixels outside the image and whole rows beyond the last one
-        {
-            const int pp = t >> 4, sub = t & 15;
-            float4* row = seg + (buf * PCH + pp) * FW;
-            const bool dead = !any || p0 + pp >= np;
-            const int pre = dead ? FW : lo - qs, post = dead ? FW : hi - qs + 1;
-            for (int i = sub; i < pre; i += 16) row[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int i = post + sub; i < FW; i += 16) row[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        // order the generic-proxy stores before later bulk copies into this buffer
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        const unsigned row_bytes = any ? static_cast<unsigned>((hi - lo + 1) * sizeof(float4)) : 0u;
-        if (t < PCH && row_bytes && p0 + t < np)
-            bulk_load(seg + (buf * PCH + t) * FW + (lo - qs), plane + static_cast<long long>(p0 + t) * nq + lo,
-                      row_bytes, &bar[buf]);
-        if (t == 0) mbar_expect_tx(&bar[buf], row_bytes * max(0, min(PCH, np - p0)));
-    };
-
-    // the reference's float projection for the edge rays
-    const bool edge = live && (b == 0 || b == nd - 1);
-    const float cxf = static_cast<float>(w - 1) * 0.5f, cyf = static_cast<float>(h - 1) * 0.5f;
-    const float dcs = static_cast<float>(nd / 2);
-
-    float4 acc[GMAX];
-#pragma unroll
-    for (int j = 0; j < GMAX; ++j) acc[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-
-    issue(0, 0);
-    __syncthreads();
-    bool ok_all = true;
-    for (int ci = 0; ci < nch; ++ci) {
-        const int buf = ci & 1;
-        if (ci + 1 < nch) issue(ci + 1, (ci + 1) & 1);
-        const bool landed = mbar_wait_bounded(&bar[buf], (ci >> 1) & 1, err);
-        const int p0 = p_lo + ci * PCH;
-        const int qs = qs_tab[ci];
-        const float4* sg = seg + buf * PCH * FW;
-        if (live) {
-#pragma unroll
-            for (int j = 0; j < GMAX; ++j) {
-                if (j >= cnt) break;
-                const FAngle f = fa[j];
-                // crossing of this ray at p0, relative to the staged segment
-                const double qstar = fma(static_cast<double>(p0), f.dq, fma(static_cast<double>(t), f.inv, f.q0b0));
-                const double qfl = floor(qstar);
-                const float lq0 = static_cast<float>(static_cast<int>(qfl) - qs) + static_cast<float>(qstar - qfl);
-#pragma unroll
-                for (int pp = 0; pp < PCH; ++pp) {
-                    const float qf = fmaf(static_cast<float>(pp), f.dqf, lq0);
-                    const float qa = ceilf(qf - f.R);
-                    const int ia = static_cast<int>(qa);
-                    const float t0 = (qa - qf) * f.kqf;  // s - b at candidate qa
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const float tt = fmaf(static_cast<float>(k), f.kqf, t0);
-                        float wgt = fmaxf(0.0f, 1.0f - fabsf(tt));
-                        if (edge) {
-                            // SerialBackend.cpp:109-120 on the reference's float s
-                            const int qg = qs + ia + k;
-                            const int pg = p0 + pp;
-                            const float xg = static_cast<float>(rows ? qg : pg);
-                            const float yg = static_cast<float>(rows ? pg : qg);
-                            const float ss = __fadd_rn(__fadd_rn(__fmul_rn(__fsub_rn(xg, cxf), f.cf),
-                                                                 __fmul_rn(__fsub_rn(yg, cyf), f.sf)), dcs);
-                            const int i0 = static_cast<int>(floorf(ss));
-                            wgt = 0.0f;
-                            if (i0 >= 0 && i0 < nd - 1) {
-                                if (i0 == b) wgt = 1.0f - tt;
-                                else if (i0 + 1 == b) wgt = 1.0f + tt;
-                            } else if (i0 == nd - 1 && b == nd - 1) {
-                                wgt = 1.0f;
-                            }
-                            wgt = fminf(fmaxf(wgt, 0.0f), 1.0f);
-                        }
-                        const float4 v = sg[pp * FW + ia + k];
-                        acc[j].x = fmaf(wgt, v.x, acc[j].x);
-                        acc[j].y = fmaf(wgt, v.y, acc[j].y);
-                        acc[j].z = fmaf(wgt, v.z, acc[j].z);
-                        acc[j].w = fmaf(wgt, v.w, acc[j].w);
-                    }
-                }
-            }
-        }
-        if (!__syncthreads_and(landed)) { ok_all = false; break; }
-    }
-    if (!ok_all || !live) return;
-#pragma unroll
-    for (int j = 0; j < GMAX; ++j) {
-        if (j >= cnt) break;
-        const float r[4] = {acc[j].x, acc[j].y, acc[j].z, acc[j].w};
-        const long long a = fa[j].a;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int z = 4 * g + k;
-            if (z < nz) sino[(static_cast<long long>(z) * na + a) * nd + b] = r[k];
-        }
-    }
-}
-
 }  // namespace
 
 cudaError_t launch_trig(const float* d_angles_deg, int na, double2* d_cs, cudaStream_t st) {
@@ -414,22 +126,6 @@ cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const flo
                              float4* d_img, float4* d_imgT, cudaStream_t st) {
     const dim3 grid((w + 31) / 32, (h + 31) / 32, (nz + 3) / 4);
     k_normalize<<<grid, 256, 0, st>>>(d_vol, w, h, nz, d_stats, d_img, d_imgT);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
-                           int na, int nd, Trig trig, const int4* d_groups, int ngroups,
-                           const int* d_order, float* d_sino, unsigned* d_err, cudaStream_t st) {
-    const size_t smem = sizeof(float4) * FNB * PCH * FW + 16 + sizeof(FAngle) * GMAX +
-                        sizeof(int) * MAXCH;
-    const cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    const int np = w > h ? w : h;
-    if ((np + PCH - 1) / PCH + 1 > MAXCH) return cudaErrorInvalidValue;
-    const dim3 grid((nd + FB - 1) / FB, ngroups, (nz + 3) / 4);
-    k_forward<<<grid, FB, smem, st>>>(d_img, d_imgT, w, h, nz, na, nd, trig, d_groups, d_order,
-                                      d_sino, d_err);
     return cudaGetLastError();
 }
 
