@@ -247,9 +247,17 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
                          const float* angles_deg, float* d_sino, float4* d_stats,
                          cudaEvent_t* ev = nullptr) {
     const int nzg = (nz + 3) / 4;
-    const size_t img = static_cast<size_t>(nzg) * w * h;
-    CTB_WS(ctx, d_img, float4, "img", img);
-    CTB_WS(ctx, d_imgT, float4, "imgT", img);
+    const size_t elems = static_cast<size_t>(nzg) * std::max(fwd_plane_elems(h, w), fwd_plane_elems(w, h));
+    CTB_WS(ctx, d_img, float4, "img", elems);
+    CTB_WS(ctx, d_imgT, float4, "imgT", elems);
+    // zero borders: cleared whenever the buffers or the plane geometry change
+    const std::vector<long long> geom = {reinterpret_cast<long long>(d_img),
+                                         reinterpret_cast<long long>(d_imgT), w, h, nzg};
+    if (ctx->img_border_geom != geom) {
+        CTB_CUDA(ctx, cudaMemsetAsync(d_img, 0, sizeof(float4) * elems, ctx->stream));
+        CTB_CUDA(ctx, cudaMemsetAsync(d_imgT, 0, sizeof(float4) * elems, ctx->stream));
+        ctx->img_border_geom = geom;
+    }
     Trig trig;
     CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
     CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream));

@@ -71,6 +71,13 @@ constexpr int kFwdRays = 128;   // rays (detector bins) per CTA
 constexpr int kFwdRows = 8;     // walked rows per staged chunk
 constexpr int kFwdWidth = 256;  // staged pixels per row
 constexpr int kFwdGroup = 8;    // angles per CTA
+// Zero border of the normalised image planes: kFwdGuard pixels on both sides
+// of every row (>= kFwdWidth + reach) and kFwdRows rows after the last, so a
+// staged segment never leaves the plane.
+constexpr int kFwdGuard = 264;
+inline size_t fwd_plane_elems(int np, int nq) {
+    return static_cast<size_t>(np + kFwdRows) * static_cast<size_t>(nq + 2 * kFwdGuard);
+}
 struct FwdPlan {
     std::vector<int> order;
     std::vector<int> groups;  // 4 ints per group
@@ -125,6 +132,7 @@ struct ctb_ctx {
         int ngroups = 0;
     };
     std::map<std::vector<long long>, FwdPlanDev> fwd_plans;
+    std::vector<long long> img_border_geom;  // geometry the image borders were zeroed for
     unsigned* d_err = nullptr;  // device error word for bounded waits
 
     // Stage profiling: a ring of event sets, one set per volume reconstruction.

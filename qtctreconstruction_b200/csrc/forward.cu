@@ -67,10 +67,15 @@ __global__ void __launch_bounds__(1024) k_slice_stats(const float* __restrict__ 
 // --------------------------------------------------------------- normalise
 // img[zg][y][x] = (v(4zg), v(4zg+1), v(4zg+2), v(4zg+3)) and imgT[zg][x][y], with
 // v = (raw - min) * (1 / span_fwd) for raw != 0 and v = 0 for raw == 0: the
-// reference skips background pixels (SerialBackend.cpp:104-106).
+// reference skips background pixels (SerialBackend.cpp:104-106). Both copies
+// use the zero-bordered layout of the projector (kFwdGuard pixels left and
+// right of every row, kFwdRows rows below the last); only the interior is
+// written here, the borders are zeroed when the buffers are set up.
 __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol, int w, int h, int nz,
                                                    const float4* __restrict__ stats,
                                                    float4* __restrict__ img, float4* __restrict__ imgT) {
+    const long long pw = w + 2 * kFwdGuard, ph = h + 2 * kFwdGuard;  // row pitches
+    const long long rw = h + kFwdRows, rh = w + kFwdRows;             // rows per plane
     __shared__ float4 tile[32][33];
     const int zg = blockIdx.z;
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
@@ -99,13 +104,13 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
         }
         const float4 q = make_float4(v[0], v[1], v[2], v[3]);
         tile[ty + 8 * r][tx] = q;
-        if (x < w && y < h) img[(static_cast<long long>(zg) * h + y) * w + x] = q;
+        if (x < w && y < h) img[(zg * rw + y) * pw + x + kFwdGuard] = q;
     }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int x = x0 + ty + 8 * r, y = y0 + tx;
-        if (x < w && y < h) imgT[(static_cast<long long>(zg) * w + x) * h + y] = tile[tx][ty + 8 * r];
+        if (x < w && y < h) imgT[(zg * rh + x) * ph + y + kFwdGuard] = tile[tx][ty + 8 * r];
     }
 }
 

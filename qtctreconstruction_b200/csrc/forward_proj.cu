@@ -18,8 +18,11 @@
 // step crosses at most three pixels of the gathered axis. Rows are processed
 // in chunks of PCH = 8; per chunk the row segments that any ray of any angle
 // of the CTA can touch (FW pixels per row) are staged once into shared memory
-// by the bulk-copy engine, double-buffered on mbarriers, with zeros where a
-// segment leaves the image, and read by all eight angles. The host forms the
+// by the bulk-copy engine and read by all eight angles. The image planes carry
+// a zero border (kFwdGuard), so a segment never needs filling. Staging is a
+// producer/consumer pipeline: two buffers, each with a "full" mbarrier (bytes
+// landed) and an "empty" mbarrier (all 16 warps done), so warps never wait on
+// one another at a CTA-wide barrier. The host forms the
 // groups so that the segment width provably fits (forward_plan). The crossing
 // point q*(b, p) is evaluated in double once per chunk and angle and split
 // into an integer and a float fraction; within the chunk each thread steps in
@@ -65,6 +68,9 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
     unsigned ok;
     asm volatile(
@@ -92,6 +98,7 @@ struct FAngle {
     float cf, sf;  // the reference's float cos/sin
     int a;
     int p_lo, p_hi;
+    int edge;  // an edge ray (bin 0 or nd-1) of this CTA reaches the image at this angle
 };
 
 // The fast path: tent weights of the (up to three) pixels around the crossing.
@@ -100,6 +107,11 @@ __device__ __forceinline__ void walk_chunk(const float4* __restrict__ sg, const 
     const double qstar = fma(static_cast<double>(p0), f.dq, fma(static_cast<double>(t), f.inv, f.q0b0));
     const double qfl = floor(qstar);
     const float lq0 = static_cast<float>(static_cast<int>(qfl) - qs) + static_cast<float>(qstar - qfl);
+    // Every crossing of every ray of the CTA lies in [3, FW - 6] of the segment
+    // unless the chunk meets no ray at all (segment start clamped to the
+    // plane); never index outside the segment in that case.
+    if (!(lq0 + fminf(0.0f, (PCH - 1) * f.dqf) >= 1.5f && lq0 + fmaxf(0.0f, (PCH - 1) * f.dqf) <= FW - 3.0f))
+        return;
 #pragma unroll
     for (int pp = 0; pp < PCH; ++pp) {
         const float qf = fmaf(static_cast<float>(pp), f.dqf, lq0);
@@ -129,6 +141,8 @@ __device__ __noinline__ void walk_chunk_edge(const float4* __restrict__ sg, cons
     const double qstar = fma(static_cast<double>(p0), f.dq, fma(static_cast<double>(t), f.inv, f.q0b0));
     const double qfl = floor(qstar);
     const float lq0 = static_cast<float>(static_cast<int>(qfl) - qs) + static_cast<float>(qstar - qfl);
+    if (!(lq0 + fminf(0.0f, (PCH - 1) * f.dqf) >= 1.5f && lq0 + fmaxf(0.0f, (PCH - 1) * f.dqf) <= FW - 3.0f))
+        return;
     const bool edge = (b == 0 || b == nd - 1);
     const float dcs = static_cast<float>(nd / 2);
     for (int pp = 0; pp < PCH; ++pp) {
@@ -175,9 +189,10 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float4* seg = reinterpret_cast<float4*>(smem_raw);  // [FNB][PCH][FW]
     unsigned char* tail = smem_raw + sizeof(float4) * FNB * PCH * FW;
-    auto bar = reinterpret_cast<unsigned long long*>(tail);
-    auto fa = reinterpret_cast<FAngle*>(tail + 16);
-    auto qs_tab = reinterpret_cast<int*>(tail + 16 + sizeof(FAngle) * GMAX);
+    auto full = reinterpret_cast<unsigned long long*>(tail);
+    auto empty = full + FNB;
+    auto fa = reinterpret_cast<FAngle*>(tail + 32);
+    auto qs_tab = reinterpret_cast<int*>(tail + 32 + sizeof(FAngle) * GMAX);
 
     const int b0 = blockIdx.x * FB;
     const int b1 = min(b0 + FB, nd);  // exclusive
@@ -187,6 +202,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     const int g = blockIdx.z;  // slice group (4 slices)
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int tid = ty * FB + tx;
+    const int lane = tid & 31;
     const int b = b0 + tx;
 
     const int np = rows ? h : w;  // walked axis
@@ -194,6 +210,20 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     const double cq = rows ? 0.5 * (w - 1) : 0.5 * (h - 1);
     const double cp = rows ? 0.5 * (h - 1) : 0.5 * (w - 1);
     const double dcf = static_cast<double>(nd / 2);
+
+    // p range of a ray family [qa, qb] (crossings at p = 0) within reach of the image
+    auto prange = [&](double qa, double qb, double dq, double reach, int& lo, int& hi) {
+        lo = 0;
+        hi = np - 1;
+        if (dq != 0.0) {
+            const double pa0 = (-reach - qa) / dq, pb0 = (nq - 1 + reach - qa) / dq;
+            const double pa1 = (-reach - qb) / dq, pb1 = (nq - 1 + reach - qb) / dq;
+            lo = max(0, static_cast<int>(floor(fmin(fmin(pa0, pb0), fmin(pa1, pb1)))) - 1);
+            hi = min(np - 1, static_cast<int>(ceil(fmax(fmax(pa0, pb0), fmax(pa1, pb1)))) + 1);
+        } else if (fmax(qa, qb) < -reach || fmin(qa, qb) > nq - 1 + reach) {
+            hi = -1;
+        }
+    };
 
     if (tid < cnt) {
         const int a = order[grp.x + tid];
@@ -212,24 +242,23 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
         f.cf = tf.x;
         f.sf = tf.y;
         f.a = a;
-        // walked range whose crossings lie within reach of the image, over the CTA's rays
         const double reach = fabs(f.inv) + 2.0;
-        const double qb1 = f.q0b0 + (b1 - 1 - b0) * f.inv;
-        int lo = 0, hi = np - 1;
-        if (f.dq != 0.0) {
-            const double pa0 = (-reach - f.q0b0) / f.dq, pb0 = (nq - 1 + reach - f.q0b0) / f.dq;
-            const double pa1 = (-reach - qb1) / f.dq, pb1 = (nq - 1 + reach - qb1) / f.dq;
-            lo = max(0, static_cast<int>(floor(fmin(fmin(pa0, pb0), fmin(pa1, pb1)))) - 1);
-            hi = min(np - 1, static_cast<int>(ceil(fmax(fmax(pa0, pb0), fmax(pa1, pb1)))) + 1);
-        } else if (fmax(f.q0b0, qb1) < -reach || fmin(f.q0b0, qb1) > nq - 1 + reach) {
-            hi = -1;
+        prange(f.q0b0, f.q0b0 + (b1 - 1 - b0) * f.inv, f.dq, reach, f.p_lo, f.p_hi);
+        f.edge = 0;
+        for (int eb : {0, nd - 1}) {
+            if (eb < b0 || eb >= b1) continue;
+            const double qe = f.q0b0 + (eb - b0) * f.inv;
+            int lo, hi;
+            prange(qe, qe, f.dq, reach, lo, hi);
+            if (hi >= lo) f.edge = 1;
         }
-        f.p_lo = lo;
-        f.p_hi = hi;
         fa[tid] = f;
     }
     if (tid == 0) {
-        for (int i = 0; i < FNB; ++i) mbar_init(&bar[i], 1);
+        for (int i = 0; i < FNB; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], THREADS / 32);
+        }
         mbar_fence_init();
     }
     __syncthreads();
@@ -254,7 +283,8 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
         return;
     }
     const int nch = (p_hi - p_lo + PCH) / PCH;
-    // first staged pixel of every chunk: minimum crossing over angles and corners
+    // first staged pixel of every chunk: minimum crossing over angles and corners,
+    // kept inside the zero-bordered plane
     for (int ci = tid; ci < nch; ci += THREADS) {
         const double p0 = p_lo + ci * PCH;
         double m = 1e300;
@@ -264,65 +294,72 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
             const double e = (PCH - 1) * fa[j].dq;
             m = fmin(m, fmin(fmin(qa0, qa1), fmin(qa0 + e, qa1 + e)));
         }
-        qs_tab[ci] = static_cast<int>(floor(m)) - 3;
+        const int qs = static_cast<int>(fmax(floor(m), -1e9)) - 3;
+        qs_tab[ci] = min(max(qs, -kFwdGuard), nq + kFwdGuard - FW);
     }
     __syncthreads();
 
-    const long long plane_sz = static_cast<long long>(np) * nq;
-    const float4* plane = (rows ? img : imgT) + static_cast<long long>(g) * plane_sz;
+    const long long pitch = nq + 2 * kFwdGuard;
+    const float4* plane = (rows ? img : imgT) + static_cast<long long>(g) * (np + PCH) * pitch + kFwdGuard;
 
+    // producer (thread 0): stage chunk ci into buffer buf; rows p0..p0+7 exist
+    // in the bordered plane, every row copy is FW pixels
     auto issue = [&](int ci, int buf) {
         const int p0 = p_lo + ci * PCH;
         const int qs = qs_tab[ci];
-        const int lo = max(qs, 0), hi = min(qs + FW - 1, nq - 1);  // in-image part
-        const bool any = hi >= lo;
-        // zero the staged pixels outside the image and whole rows beyond the last one
-        {
-            const int pp = tid / (THREADS / PCH), sub = tid % (THREADS / PCH);
-            constexpr int STRIDE = THREADS / PCH;
-            float4* row = seg + (buf * PCH + pp) * FW;
-            const bool dead = !any || p0 + pp >= np;
-            const int pre = dead ? FW : lo - qs, post = dead ? FW : hi - qs + 1;
-            for (int i = sub; i < pre; i += STRIDE) row[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int i = post + sub; i < FW; i += STRIDE) row[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        // order the generic-proxy stores before later bulk copies into this buffer
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        const unsigned row_bytes = any ? static_cast<unsigned>((hi - lo + 1) * sizeof(float4)) : 0u;
-        if (tid < PCH && row_bytes && p0 + tid < np)
-            bulk_load(seg + (buf * PCH + tid) * FW + (lo - qs),
-                      plane + static_cast<long long>(p0 + tid) * nq + lo, row_bytes, &bar[buf]);
-        if (tid == 0) mbar_expect_tx(&bar[buf], row_bytes * max(0, min(PCH, np - p0)));
+        mbar_expect_tx(&full[buf], PCH * FW * sizeof(float4));
+        for (int r = 0; r < PCH; ++r)
+            bulk_load(seg + (buf * PCH + r) * FW, plane + static_cast<long long>(p0 + r) * pitch + qs,
+                      FW * sizeof(float4), &full[buf]);
     };
 
-    // warps holding an edge ray take the path with the reference's edge decisions
-    const bool edge_warp = (b0 + (tx & ~31) <= 0 && 0 < b0 + (tx & ~31) + 32) ||
-                           (b0 + (tx & ~31) <= nd - 1 && nd - 1 < b0 + (tx & ~31) + 32);
+    // warps holding an edge ray that meets the image take the reference-decision path
+    const int wb0 = b0 + (tx & ~31);
+    const bool holds_edge = (wb0 <= 0 && 0 < wb0 + 32) || (wb0 <= nd - 1 && nd - 1 < wb0 + 32);
+    const bool edge_a = holds_edge && has_a && fa[ja].edge;
+    const bool edge_b = holds_edge && has_b && fa[jb].edge;
     const float cxf = static_cast<float>(w - 1) * 0.5f, cyf = static_cast<float>(h - 1) * 0.5f;
 
     float4 acc_a = make_float4(0.f, 0.f, 0.f, 0.f), acc_b = acc_a;
-    issue(0, 0);
-    __syncthreads();
-    bool ok_all = true;
+    int last_issued = 0;  // producer only
+    if (tid == 0) issue(0, 0);
+    bool ok = true;
     for (int ci = 0; ci < nch; ++ci) {
         const int buf = ci & 1;
-        if (ci + 1 < nch) issue(ci + 1, (ci + 1) & 1);
-        const bool landed = mbar_wait_bounded(&bar[buf], (ci >> 1) & 1, err);
+        if (tid == 0 && ci + 1 < nch) {
+            // the next buffer last held chunk ci-1: wait until all warps released it
+            const int nb = (ci + 1) & 1;
+            if (ci >= 1 && !mbar_wait_bounded(&empty[nb], ((ci - 1) >> 1) & 1, err)) ok = false;
+            if (ok) {
+                issue(ci + 1, nb);
+                last_issued = ci + 1;
+            }
+        }
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0 && ok;
+        if (!ok || !mbar_wait_bounded(&full[buf], (ci >> 1) & 1, err)) { ok = false; break; }
         const int p0 = p_lo + ci * PCH;
         const int qs = qs_tab[ci];
         const float4* sg = seg + buf * PCH * FW;
         if (live) {
-            if (!edge_warp) {
-                if (has_a) walk_chunk(sg, fa[ja], tx, p0, qs, acc_a);
-                if (has_b) walk_chunk(sg, fa[jb], tx, p0, qs, acc_b);
-            } else {
-                if (has_a) walk_chunk_edge(sg, fa[ja], tx, p0, qs, b, nd, rows, cxf, cyf, acc_a);
-                if (has_b) walk_chunk_edge(sg, fa[jb], tx, p0, qs, b, nd, rows, cxf, cyf, acc_b);
+            if (has_a) {
+                if (edge_a) walk_chunk_edge(sg, fa[ja], tx, p0, qs, b, nd, rows, cxf, cyf, acc_a);
+                else walk_chunk(sg, fa[ja], tx, p0, qs, acc_a);
+            }
+            if (has_b) {
+                if (edge_b) walk_chunk_edge(sg, fa[jb], tx, p0, qs, b, nd, rows, cxf, cyf, acc_b);
+                else walk_chunk(sg, fa[jb], tx, p0, qs, acc_b);
             }
         }
-        if (!__syncthreads_and(landed)) { ok_all = false; break; }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[buf]);
     }
-    if (!ok_all || !live) return;
+    if (!ok) {
+        // a bounded wait gave up: let the producer's copies in flight land (again
+        // bounded) before the CTA's shared memory is released
+        if (tid == 0) mbar_wait_bounded(&full[last_issued & 1], (last_issued >> 1) & 1, nullptr);
+        return;
+    }
+    if (!live) return;
     const float ra[4] = {acc_a.x, acc_a.y, acc_a.z, acc_a.w};
     const float rb[4] = {acc_b.x, acc_b.y, acc_b.z, acc_b.w};
 #pragma unroll
@@ -339,7 +376,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
                            int na, int nd, Trig trig, const int4* d_groups, int ngroups,
                            const int* d_order, float* d_sino, unsigned* d_err, cudaStream_t st) {
-    const size_t smem = sizeof(float4) * FNB * PCH * FW + 16 + sizeof(FAngle) * GMAX +
+    const size_t smem = sizeof(float4) * FNB * PCH * FW + 32 + sizeof(FAngle) * GMAX +
                         sizeof(int) * MAXCH;
     const cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smem));
