@@ -135,14 +135,14 @@ __device__ __forceinline__ void walk_chunk(const float4* __restrict__ sg, const 
 // The edge rays: SerialBackend.cpp:109-120 decides, on its own float s, which
 // pixels reach bins 0 and nd-1 (bin 0 only from floor(s) == 0; bin nd-1 from
 // floor(s) == nd-2 with weight frac and from floor(s) == nd-1 with weight 1).
-__device__ __noinline__ void walk_chunk_edge(const float4* __restrict__ sg, const FAngle& f, int t,
-                                             int p0, int qs, int b, int nd, bool rows, float cxf,
-                                             float cyf, float4& acc) {
+__device__ __noinline__ float4 walk_chunk_edge(const float4* __restrict__ sg, const FAngle& f, int t,
+                                               int p0, int qs, int b, int nd, bool rows, float cxf,
+                                               float cyf, float4 acc) {
     const double qstar = fma(static_cast<double>(p0), f.dq, fma(static_cast<double>(t), f.inv, f.q0b0));
     const double qfl = floor(qstar);
     const float lq0 = static_cast<float>(static_cast<int>(qfl) - qs) + static_cast<float>(qstar - qfl);
     if (!(lq0 + fminf(0.0f, (PCH - 1) * f.dqf) >= 1.5f && lq0 + fmaxf(0.0f, (PCH - 1) * f.dqf) <= FW - 3.0f))
-        return;
+        return acc;
     const bool edge = (b == 0 || b == nd - 1);
     const float dcs = static_cast<float>(nd / 2);
     for (int pp = 0; pp < PCH; ++pp) {
@@ -177,6 +177,7 @@ __device__ __noinline__ void walk_chunk_edge(const float4* __restrict__ sg, cons
             acc.w = fmaf(wgt, v.w, acc.w);
         }
     }
+    return acc;
 }
 
 __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict__ img,
@@ -342,11 +343,11 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
         const float4* sg = seg + buf * PCH * FW;
         if (live) {
             if (has_a) {
-                if (edge_a) walk_chunk_edge(sg, fa[ja], tx, p0, qs, b, nd, rows, cxf, cyf, acc_a);
+                if (edge_a) acc_a = walk_chunk_edge(sg, fa[ja], tx, p0, qs, b, nd, rows, cxf, cyf, acc_a);
                 else walk_chunk(sg, fa[ja], tx, p0, qs, acc_a);
             }
             if (has_b) {
-                if (edge_b) walk_chunk_edge(sg, fa[jb], tx, p0, qs, b, nd, rows, cxf, cyf, acc_b);
+                if (edge_b) acc_b = walk_chunk_edge(sg, fa[jb], tx, p0, qs, b, nd, rows, cxf, cyf, acc_b);
                 else walk_chunk(sg, fa[jb], tx, p0, qs, acc_b);
             }
         }
