@@ -32,6 +32,8 @@ constexpr int WIN = kBpWindow;
 constexpr int CA = 32;        // angles per chunk
 constexpr int NBUF = 2;       // chunk buffers
 constexpr int THREADS = 256;  // 8 (x) x 32 (y) threads, 4 x-positions each
+constexpr float kRound = 12582912.0f;   // 1.5 * 2^23: x + kRound rounds x to an integer
+constexpr int kRoundBits = 0x4B400000;  // bit pattern of kRound
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -187,13 +189,18 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
             const float ub = fmaf(fx, r.c, fmaf(-fy, r.s, r.f0));
             const float c8 = 8.0f * r.c;
             if (!r.edge) {
+                // i = floor(u) by rounding u - 1/2 with the kRound addition (no
+                // conversion-unit instructions); at an exact tie u = i + 1 the taps
+                // shift to (i, i+1) with weights (0, 1), the same value
+                const float ubh = ub - 0.5f;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    const float u = fmaf(static_cast<float>(k), c8, ub);
-                    const float fl = floorf(u);
-                    const int i = static_cast<int>(fl);
-                    const float w1 = u - fl;
-                    const float w0 = 1.0f - w1;
+                    const float uh = fmaf(static_cast<float>(k), c8, ubh);
+                    const float tr = uh + kRound;
+                    const int i = __float_as_int(tr) - kRoundBits;
+                    const float d = uh - (tr - kRound);  // frac(u) - 1/2
+                    const float w1 = d + 0.5f;
+                    const float w0 = 0.5f - d;
                     const float4 lo = w[i], hi = w[i + 1];
                     acc[k].x = fmaf(w1, hi.x, fmaf(w0, lo.x, acc[k].x));
                     acc[k].y = fmaf(w1, hi.y, fmaf(w0, lo.y, acc[k].y));

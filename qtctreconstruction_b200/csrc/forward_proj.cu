@@ -43,8 +43,10 @@ constexpr int FW = kFwdWidth;
 constexpr int GMAX = kFwdGroup;
 constexpr int AY = 4;            // angle lanes per CTA (each thread: angles y, y + AY)
 constexpr int THREADS = FB * AY;
-constexpr int FNB = 2;           // chunk buffers
+constexpr int FNB = 3;           // chunk buffers (pipeline depth)
 constexpr int MAXCH = 512;       // chunk table capacity (walked extent <= 4096)
+constexpr float kRound = 12582912.0f;  // 1.5 * 2^23: x + kRound rounds x to an integer
+constexpr int kRoundBits = 0x4B400000;  // bit pattern of kRound
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -95,6 +97,7 @@ struct FAngle {
     double inv;   // dq*/db = 1 / kq
     double dq;    // dq*/dp = -kp / kq
     float kqf, R, dqf;
+    float cr;      // 0.5 - R: ceil(q - R) = round-to-nearest(q + 0.5 - R) via kRound
     float cf, sf;  // the reference's float cos/sin
     int a;
     int p_lo, p_hi;
@@ -115,8 +118,12 @@ __device__ __forceinline__ void walk_chunk(const float4* __restrict__ sg, const 
 #pragma unroll
     for (int pp = 0; pp < PCH; ++pp) {
         const float qf = fmaf(static_cast<float>(pp), f.dqf, lq0);
-        const float qa = ceilf(qf - f.R);
-        const int ia = static_cast<int>(qa);
+        // first candidate ceil(qf - R), rounded by adding 1.5 * 2^23 (FADD and an
+        // integer subtract instead of conversion-unit instructions); a tie moves
+        // the three candidates by one pixel at distance exactly R (weight 0)
+        const float tr = (qf + f.cr) + kRound;
+        const int ia = __float_as_int(tr) - kRoundBits;
+        const float qa = tr - kRound;
         const float t0 = (qa - qf) * f.kqf;  // s - b at candidate qa
         const float4* row = sg + pp * FW + ia;
 #pragma unroll
@@ -192,8 +199,8 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     unsigned char* tail = smem_raw + sizeof(float4) * FNB * PCH * FW;
     auto full = reinterpret_cast<unsigned long long*>(tail);
     auto empty = full + FNB;
-    auto fa = reinterpret_cast<FAngle*>(tail + 32);
-    auto qs_tab = reinterpret_cast<int*>(tail + 32 + sizeof(FAngle) * GMAX);
+    auto fa = reinterpret_cast<FAngle*>(tail + 16 * FNB);
+    auto qs_tab = reinterpret_cast<int*>(tail + 16 * FNB + sizeof(FAngle) * GMAX);
 
     const int b0 = blockIdx.x * FB;
     const int b1 = min(b0 + FB, nd);  // exclusive
@@ -238,6 +245,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
         f.q0b0 = cq + (static_cast<double>(b0) - dcf + cp * kp) * f.inv;
         f.kqf = static_cast<float>(kq);
         f.R = static_cast<float>(fabs(f.inv));
+        f.cr = 0.5f - f.R;
         f.dqf = static_cast<float>(f.dq);
         const float2 tf = trig.csf[a];
         f.cf = tf.x;
@@ -322,22 +330,27 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     const float cxf = static_cast<float>(w - 1) * 0.5f, cyf = static_cast<float>(h - 1) * 0.5f;
 
     float4 acc_a = make_float4(0.f, 0.f, 0.f, 0.f), acc_b = acc_a;
-    int last_issued = 0;  // producer only
-    if (tid == 0) issue(0, 0);
+    int last_issued = -1;  // producer only
+    if (tid == 0)
+        for (int ci = 0; ci < FNB - 1 && ci < nch; ++ci) {
+            issue(ci, ci);
+            last_issued = ci;
+        }
     bool ok = true;
     for (int ci = 0; ci < nch; ++ci) {
-        const int buf = ci & 1;
-        if (tid == 0 && ci + 1 < nch) {
-            // the next buffer last held chunk ci-1: wait until all warps released it
-            const int nb = (ci + 1) & 1;
-            if (ci >= 1 && !mbar_wait_bounded(&empty[nb], ((ci - 1) >> 1) & 1, err)) ok = false;
+        const int buf = ci % FNB;
+        const int nxt = ci + FNB - 1;
+        if (tid == 0 && nxt < nch) {
+            // the buffer of chunk nxt last held chunk ci-1: wait until all warps released it
+            const int nb = nxt % FNB;
+            if (ci >= 1 && !mbar_wait_bounded(&empty[nb], ((ci - 1) / FNB) & 1, err)) ok = false;
             if (ok) {
-                issue(ci + 1, nb);
-                last_issued = ci + 1;
+                issue(nxt, nb);
+                last_issued = nxt;
             }
         }
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0 && ok;
-        if (!ok || !mbar_wait_bounded(&full[buf], (ci >> 1) & 1, err)) { ok = false; break; }
+        if (!ok || !mbar_wait_bounded(&full[buf], (ci / FNB) & 1, err)) { ok = false; break; }
         const int p0 = p_lo + ci * PCH;
         const int qs = qs_tab[ci];
         const float4* sg = seg + buf * PCH * FW;
@@ -357,7 +370,8 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     if (!ok) {
         // a bounded wait gave up: let the producer's copies in flight land (again
         // bounded) before the CTA's shared memory is released
-        if (tid == 0) mbar_wait_bounded(&full[last_issued & 1], (last_issued >> 1) & 1, nullptr);
+        if (tid == 0 && last_issued >= 0)
+            mbar_wait_bounded(&full[last_issued % FNB], (last_issued / FNB) & 1, nullptr);
         return;
     }
     if (!live) return;
@@ -377,7 +391,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
                            int na, int nd, Trig trig, const int4* d_groups, int ngroups,
                            const int* d_order, float* d_sino, unsigned* d_err, cudaStream_t st) {
-    const size_t smem = sizeof(float4) * FNB * PCH * FW + 32 + sizeof(FAngle) * GMAX +
+    const size_t smem = sizeof(float4) * FNB * PCH * FW + 16 * FNB + sizeof(FAngle) * GMAX +
                         sizeof(int) * MAXCH;
     const cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smem));
