@@ -172,6 +172,17 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
 #pragma unroll
     for (int k = 0; k < 4; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
     const float fx = static_cast<float>(lx), fy = static_cast<float>(ly);
+    // positions inside the reconstruction circle (SerialBackend.cpp:220-224);
+    // the others are written as the offset only, so their taps are never loaded
+    unsigned inside_mask = 0;
+    {
+        const float yy = static_cast<float>(y0 + ly) - radf;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float xx = static_cast<float>(x0 + lx + 8 * k) - radf;
+            if (!(xx * xx + yy * yy > radf * radf)) inside_mask |= 1u << k;
+        }
+    }
 
     issue(0, 0);
     __syncthreads();
@@ -195,6 +206,7 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
                 const float ubh = ub - 0.5f;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
+                    if (!(inside_mask & (1u << k))) continue;
                     const float uh = fmaf(static_cast<float>(k), c8, ubh);
                     const float tr = uh + kRound;
                     const int i = __float_as_int(tr) - kRoundBits;
@@ -214,6 +226,7 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
                 // here exactly, the interpolation itself uses the accurate u.
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
+                    if (!(inside_mask & (1u << k))) continue;
                     const float u = fmaf(static_cast<float>(k), c8, ub);
                     const float fl = floorf(u);
                     const int i = static_cast<int>(fl);

@@ -155,40 +155,38 @@ ctb_status trig_table(ctb_ctx* ctx, const float* angles_deg, int na, Trig* out) 
     return CTB_OK;
 }
 
-// Filter spectrum for the complex-pair FFT: Hs[k] = H[min(k, L-k)] / L with
-// Hs[0] = Hs[L/2] = 0 (the reference's inverse transform drops the Nyquist bin).
-ctb_status filter_tables(ctb_ctx* ctx, int L, int type, const float** d_Hs, const float2** d_tw) {
-    auto key = std::make_pair(L, type);
+// Convolution spectrum (conv_response) per (fft size, filter, bins), and the
+// twiddle table exp(-2 pi i k / Lc) per convolution length.
+ctb_status filter_tables(ctb_ctx* ctx, const PadGeom& g, int type, const float2** d_Hc,
+                         const float2** d_tw) {
+    const int Lc = g.Lc;
+    auto key = std::make_pair(g.bins, type);
     auto it = ctx->filters.find(key);
     if (it == ctx->filters.end()) {
-        const std::vector<double> H = filter_response(L, type);
-        std::vector<float> Hs(L);
-        for (int k = 0; k < L; ++k) {
-            const int m = k <= L / 2 ? k : L - k;
-            Hs[k] = static_cast<float>(H[m] / L);
-        }
-        Hs[0] = 0.0f;
-        Hs[L / 2] = 0.0f;
+        const std::vector<double> Hd = conv_response(g, type);
+        std::vector<float2> Hc(Lc);
+        for (int k = 0; k < Lc; ++k)
+            Hc[k] = make_float2(static_cast<float>(Hd[2 * k]), static_cast<float>(Hd[2 * k + 1]));
         DevBuf b;
-        CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float) * L));
-        b.bytes = sizeof(float) * L;
-        CTB_CUDA(ctx, cudaMemcpy(b.ptr, Hs.data(), b.bytes, cudaMemcpyHostToDevice));
+        CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float2) * Lc));
+        b.bytes = sizeof(float2) * Lc;
+        CTB_CUDA(ctx, cudaMemcpy(b.ptr, Hc.data(), b.bytes, cudaMemcpyHostToDevice));
         it = ctx->filters.emplace(key, b).first;
     }
-    auto jt = ctx->twiddles.find(L);
+    auto jt = ctx->twiddles.find(Lc);
     if (jt == ctx->twiddles.end()) {
-        std::vector<float2> tw(L);
-        for (int i = 0; i < L; ++i) {
-            const double ang = 2.0 * 3.14159265358979323846 * static_cast<double>(i) / L;
+        std::vector<float2> tw(Lc);
+        for (int i = 0; i < Lc; ++i) {
+            const double ang = 2.0 * 3.14159265358979323846 * static_cast<double>(i) / Lc;
             tw[i] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(-std::sin(ang)));
         }
         DevBuf b;
-        CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float2) * L));
-        b.bytes = sizeof(float2) * L;
+        CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float2) * Lc));
+        b.bytes = sizeof(float2) * Lc;
         CTB_CUDA(ctx, cudaMemcpy(b.ptr, tw.data(), b.bytes, cudaMemcpyHostToDevice));
-        jt = ctx->twiddles.emplace(L, b).first;
+        jt = ctx->twiddles.emplace(Lc, b).first;
     }
-    *d_Hs = static_cast<const float*>(it->second.ptr);
+    *d_Hc = static_cast<const float2*>(it->second.ptr);
     *d_tw = static_cast<const float2*>(jt->second.ptr);
     return CTB_OK;
 }
@@ -276,19 +274,20 @@ ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins
                      const float* angles_deg, int n_out, int filter, const float4* d_stats,
                      int denorm, float* d_out, cudaEvent_t* ev = nullptr) {
     const PadGeom g = pad_geometry(bins);
-    if (g.L > kMaxFft)
-        return fail(ctx, CTB_ERR_UNSUPPORTED, "fft size %d (bins %d) exceeds %d", g.L, bins, kMaxFft);
+    if (g.Lc > kMaxFft)
+        return fail(ctx, CTB_ERR_UNSUPPORTED, "convolution length %d (bins %d) exceeds %d", g.Lc, bins,
+                    kMaxFft);
     const FiltLayout fl = filt_layout(g.sq, n_out);
     const int nzg = (nz + 3) / 4;
     CTB_WS(ctx, d_filt, float4, "filt", static_cast<size_t>(nzg) * na * fl.pitch);
-    const float* d_Hs = nullptr;
+    const float2* d_Hc = nullptr;
     const float2* d_tw = nullptr;
-    CTB_TRY(filter_tables(ctx, g.L, filter, &d_Hs, &d_tw));
+    CTB_TRY(filter_tables(ctx, g, filter, &d_Hc, &d_tw));
     Trig trig;
     CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
     // SerialBackend.cpp:246: pi / (2 na) in float
     const float scale = 3.14159265358979323846f / (2.0f * static_cast<float>(na));
-    CTB_LAUNCH(ctx, launch_filter(d_sino, nz, na, g, fl, d_Hs, d_tw, d_stats, denorm, scale, d_filt,
+    CTB_LAUNCH(ctx, launch_filter(d_sino, nz, na, g, fl, d_Hc, d_tw, d_stats, denorm, scale, d_filt,
                                   ctx->stream));
     mark(ctx, ev, 3);
     CTB_LAUNCH(ctx, launch_backproject(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out,

@@ -20,8 +20,16 @@ struct PadGeom {
     int sq = 0;    // square_bins = ceil(sqrt(2) * bins)
     int pad = 0;   // pad_before = sq/2 - bins/2
     int L = 0;     // fft_size = max(64, nextPow2(2 * sq))
+    int Lc = 0;    // convolution length used on the device: max(64, nextPow2(sq + bins - 1))
 };
 PadGeom pad_geometry(int bins);
+// The reference filters a row by circular convolution, length L, with
+// h = IDFT_L(H~) (H~[k] = H[min(k, L-k)], bins 0 and L/2 zero). Only lags
+// d in [-(pad + bins - 1), sq - 1 - pad] ever meet data, a range of sq + bins - 1
+// <= Lc samples, so the same linear operator is a circular convolution of length
+// Lc with h restricted to those lags. Returns DFT_Lc of that kernel divided by Lc
+// (re, im interleaved), evaluated in double precision.
+std::vector<double> conv_response(const PadGeom& g, int type);
 
 // Layout of the filtered rows the backprojector reads: for each group of four
 // slices and each angle, `pitch` bins of float4 (one float per slice), with
@@ -87,7 +95,7 @@ cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int
                            int na, int nd, Trig trig, const int4* d_groups, int ngroups,
                            const int* d_order, float* d_sino, unsigned* d_err, cudaStream_t st);
 cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
-                          const FiltLayout& fl, const float* d_Hs, const float2* d_tw,
+                          const FiltLayout& fl, const float2* d_Hc, const float2* d_tw,
                           const float4* d_stats, int denorm, float scale, float4* d_filt,
                           cudaStream_t st);
 cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltLayout& fl,

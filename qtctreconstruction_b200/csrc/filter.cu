@@ -190,7 +190,7 @@ __device__ __forceinline__ void first_pass(float2* buf, int L, int tid, int T, c
 template <int K>
 __device__ __forceinline__ void fused_middle(float2* buf, int L, int tid, int T,
                                              const float2* __restrict__ tw,
-                                             const float* __restrict__ Hs) {
+                                             const float2* __restrict__ Hc) {
     constexpr int NB = K;
     float2 v[NB][16];
     const int LR = L / 16;
@@ -205,11 +205,7 @@ __device__ __forceinline__ void fused_middle(float2* buf, int L, int tid, int T,
         }
         dft16<false>(v[bi]);
 #pragma unroll
-        for (int r = 0; r < 16; ++r) {
-            const float hk = __ldg(Hs + j + r * LR);
-            v[bi][r].x *= hk;
-            v[bi][r].y *= hk;
-        }
+        for (int r = 0; r < 16; ++r) v[bi][r] = cmul(v[bi][r], __ldg(Hc + j + r * LR));
         dft16<true>(v[bi]);
     }
     __syncthreads();
@@ -228,7 +224,7 @@ __device__ __forceinline__ void fused_middle(float2* buf, int L, int tid, int T,
 template <int K>
 __device__ void filter_rows(float2* buf, int L, int logL, int tid, int T, const float* r0,
                             const float* r1, int pad, int nd, const float2* __restrict__ tw,
-                            const float* __restrict__ Hs) {
+                            const float2* __restrict__ Hc) {
     const int rem = logL & 3;
     const int q = logL >> 2;  // radix-16 passes per transform (>= 1 for L >= 64)
     int Ns = 1;
@@ -241,7 +237,7 @@ __device__ void filter_rows(float2* buf, int L, int logL, int tid, int T, const 
         stockham_pass<16, false, K>(buf, L, Ns, tid, T, tw);
         Ns *= 16;
     }
-    fused_middle<K>(buf, L, tid, T, tw, Hs);
+    fused_middle<K>(buf, L, tid, T, tw, Hc);
     Ns = 16;
     for (int p = 0; p < q - 1; ++p) {
         stockham_pass<16, true, K>(buf, L, Ns, tid, T, tw);
@@ -268,7 +264,7 @@ __device__ __forceinline__ float slice_scale(const float4* stats, int z, int nz,
 template <int K>
 __global__ void __launch_bounds__(256) k_filter(const float* __restrict__ sino, int nz, int na, int nd,
                                                 int sq, int pad, int L, int logL, int guard, int pitch,
-                                                const float* __restrict__ Hs,
+                                                const float2* __restrict__ Hc,
                                                 const float2* __restrict__ tw,
                                                 const float4* __restrict__ stats, int denorm,
                                                 float scale, float4* __restrict__ filt) {
@@ -279,7 +275,7 @@ __global__ void __launch_bounds__(256) k_filter(const float* __restrict__ sino, 
     const int tid = threadIdx.x;
     const float* r0 = sino + (static_cast<long long>(z0) * na + a) * nd;
     const float* r1 = z1 < nz ? sino + (static_cast<long long>(z1) * na + a) * nd : nullptr;
-    filter_rows<K>(smem, L, logL, tid, T, r0, r1, pad, nd, tw, Hs);
+    filter_rows<K>(smem, L, logL, tid, T, r0, r1, pad, nd, tw, Hc);
     const float s0 = slice_scale(stats, z0, nz, denorm, scale);
     const float s1 = slice_scale(stats, z1, nz, denorm, scale);
     // rows z0, z1 are lanes (z0 % 4, z0 % 4 + 1) of the float4 layout
@@ -299,21 +295,22 @@ __global__ void __launch_bounds__(256) k_filter(const float* __restrict__ sino, 
 }  // namespace
 
 cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
-                          const FiltLayout& fl, const float* d_Hs, const float2* d_tw,
+                          const FiltLayout& fl, const float2* d_Hc, const float2* d_tw,
                           const float4* d_stats, int denorm, float scale, float4* d_filt,
                           cudaStream_t st) {
+    const int L = g.Lc;
     int logL = 0;
-    while ((1 << logL) < g.L) ++logL;
-    const int K = g.L > 4096 ? 2 : 1;
-    const int threads = g.L / (16 * K);
-    const size_t smem = static_cast<size_t>(g.L + (g.L >> 4)) * sizeof(float2);
+    while ((1 << logL) < L) ++logL;
+    const int K = L > 4096 ? 2 : 1;
+    const int threads = L / (16 * K);
+    const size_t smem = static_cast<size_t>(L + (L >> 4)) * sizeof(float2);
     auto kern = K == 2 ? k_filter<2> : k_filter<1>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     const dim3 grid(na, (nz + 1) / 2);
-    kern<<<grid, threads, smem, st>>>(d_sino, nz, na, g.bins, g.sq, g.pad, g.L, logL, fl.guard,
-                                      fl.pitch, d_Hs, d_tw, d_stats, denorm, scale, d_filt);
+    kern<<<grid, threads, smem, st>>>(d_sino, nz, na, g.bins, g.sq, g.pad, L, logL, fl.guard,
+                                      fl.pitch, d_Hc, d_tw, d_stats, denorm, scale, d_filt);
     return cudaGetLastError();
 }
 

@@ -105,8 +105,11 @@ struct FAngle {
 };
 
 // The fast path: tent weights of the (up to three) pixels around the crossing.
+// Loads are issued only where they can matter: rows where the crossing lies
+// outside the image (plus reach) and a third candidate with weight 0 are
+// predicated off, so they cost no shared-memory bandwidth.
 __device__ __forceinline__ void walk_chunk(const float4* __restrict__ sg, const FAngle& f, int t,
-                                           int p0, int qs, float4& acc) {
+                                           int p0, int qs, int nq, float4& acc) {
     const double qstar = fma(static_cast<double>(p0), f.dq, fma(static_cast<double>(t), f.inv, f.q0b0));
     const double qfl = floor(qstar);
     const float lq0 = static_cast<float>(static_cast<int>(qfl) - qs) + static_cast<float>(qstar - qfl);
@@ -115,9 +118,12 @@ __device__ __forceinline__ void walk_chunk(const float4* __restrict__ sg, const 
     // plane); never index outside the segment in that case.
     if (!(lq0 + fminf(0.0f, (PCH - 1) * f.dqf) >= 1.5f && lq0 + fmaxf(0.0f, (PCH - 1) * f.dqf) <= FW - 3.0f))
         return;
+    // image extent in segment coordinates, widened by the tent reach
+    const float lo_img = static_cast<float>(-qs) - f.R, hi_img = static_cast<float>(nq - 1 - qs) + f.R;
 #pragma unroll
     for (int pp = 0; pp < PCH; ++pp) {
         const float qf = fmaf(static_cast<float>(pp), f.dqf, lq0);
+        if (qf < lo_img || qf > hi_img) continue;
         // first candidate ceil(qf - R), rounded by adding 1.5 * 2^23 (FADD and an
         // integer subtract instead of conversion-unit instructions); a tie moves
         // the three candidates by one pixel at distance exactly R (weight 0)
@@ -130,6 +136,7 @@ __device__ __forceinline__ void walk_chunk(const float4* __restrict__ sg, const 
         for (int k = 0; k < 3; ++k) {
             const float tt = fmaf(static_cast<float>(k), f.kqf, t0);
             const float wgt = fmaxf(0.0f, 1.0f - fabsf(tt));
+            if (k == 2 && !(wgt > 0.0f)) break;
             const float4 v = row[k];
             acc.x = fmaf(wgt, v.x, acc.x);
             acc.y = fmaf(wgt, v.y, acc.y);
@@ -357,11 +364,11 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
         if (live) {
             if (has_a) {
                 if (edge_a) acc_a = walk_chunk_edge(sg, fa[ja], tx, p0, qs, b, nd, rows, cxf, cyf, acc_a);
-                else walk_chunk(sg, fa[ja], tx, p0, qs, acc_a);
+                else walk_chunk(sg, fa[ja], tx, p0, qs, nq, acc_a);
             }
             if (has_b) {
                 if (edge_b) acc_b = walk_chunk_edge(sg, fa[jb], tx, p0, qs, b, nd, rows, cxf, cyf, acc_b);
-                else walk_chunk(sg, fa[jb], tx, p0, qs, acc_b);
+                else walk_chunk(sg, fa[jb], tx, p0, qs, nq, acc_b);
             }
         }
         __syncwarp();

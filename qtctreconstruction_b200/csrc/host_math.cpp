@@ -48,7 +48,34 @@ PadGeom pad_geometry(int bins) {
     int L = 1;
     while (L < 2 * g.sq) L <<= 1;
     g.L = std::max(64, L);
+    int Lc = 1;
+    while (Lc < g.sq + bins - 1) Lc <<= 1;
+    g.Lc = std::max(64, Lc);
     return g;
+}
+
+std::vector<double> conv_response(const PadGeom& g, int type) {
+    const int L = g.L, Lc = g.Lc;
+    const std::vector<double> H = filter_response(L, type);
+    // h = IDFT_L(H~): H~ is real and even, so h = Re FFT_L(H~) / L (real, even)
+    std::vector<std::complex<double>> t(L);
+    for (int k = 0; k < L; ++k) t[k] = H[k <= L / 2 ? k : L - k];
+    t[0] = 0.0;
+    t[L / 2] = 0.0;
+    fft64(t);
+    std::vector<std::complex<double>> hc(Lc, 0.0);
+    const int dmin = -(g.pad + g.bins - 1), dmax = g.sq - 1 - g.pad;
+    for (int d = dmin; d <= dmax; ++d) {
+        const double hv = t[((d % L) + L) % L].real() / L;
+        hc[((d % Lc) + Lc) % Lc] = hv;
+    }
+    fft64(hc);
+    std::vector<double> out(2 * static_cast<size_t>(Lc));
+    for (int k = 0; k < Lc; ++k) {
+        out[2 * k] = hc[k].real() / Lc;
+        out[2 * k + 1] = hc[k].imag() / Lc;
+    }
+    return out;
 }
 
 std::vector<double> filter_response(int L, int type) {
