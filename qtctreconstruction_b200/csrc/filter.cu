@@ -9,8 +9,11 @@
 // k = 0 and k = L/2.
 //
 // Here two real rows travel as the real and imaginary parts of one complex
-// sequence: with a real, even response the filtered rows come back as the real
-// and imaginary parts of IFFT(Hs * FFT(row0 + i row1)). A block filters the four
+// sequence: convolution with a real kernel is real-linear, so the filtered rows
+// come back as the real and imaginary parts of IFFT(Hc * FFT(row0 + i row1)).
+// The transform length is the convolution length Lc = nextPow2(sq + nd - 1)
+// (about L/2) with the restricted-lag response Hc (conv_response): the same
+// linear operator as the reference's length-L filtering. A block filters the four
 // slices of a slice group at one angle (two complex FFTs of length L in shared
 // memory, L/16 threads each). The FFT is a radix-16 Stockham transform (one
 // radix-2/4/8 pass when log2 L is not a multiple of 4) with twiddles read
@@ -116,6 +119,28 @@ __device__ __forceinline__ void dft(float2* v) {
     else dft16<INV>(v);
 }
 
+// Twiddles w[r] = exp(-+2 pi i r m / L) = tw[r m], r = 0..15, for a radix-16
+// butterfly: six table loads (r = 1, 2, 3, 4, 8, 12), the other nine as one
+// product each (w[4a + b] = w[4a] w[b]).
+template <bool INV>
+__device__ __forceinline__ void twiddles16(const float2* __restrict__ tw, int m, float2 (&w)[16]) {
+    w[0] = make_float2(1.0f, 0.0f);
+    w[1] = __ldg(tw + m);
+    w[2] = __ldg(tw + 2 * m);
+    w[3] = __ldg(tw + 3 * m);
+    w[4] = __ldg(tw + 4 * m);
+    w[8] = __ldg(tw + 8 * m);
+    w[12] = __ldg(tw + 12 * m);
+#pragma unroll
+    for (int a = 4; a <= 12; a += 4)
+#pragma unroll
+        for (int b = 1; b < 4; ++b) w[a + b] = cmul(w[a], w[b]);
+    if (INV) {
+#pragma unroll
+        for (int r = 1; r < 16; ++r) w[r].y = -w[r].y;
+    }
+}
+
 // One Stockham pass of radix R over a length-L sequence in shared memory,
 // executed by T = L/(16 K) threads (16 K / R butterflies each). Ns is the
 // length of the sub-transforms already combined. tw[i] = exp(-2 pi i i / L).
@@ -133,11 +158,18 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int L, int Ns, int ti
         for (int r = 0; r < R; ++r) v[bi][r] = buf[padi(j + r * LR)];
         if (Ns > 1) {
             const int step = L / (Ns * R);
+            if constexpr (R == 16) {
+                float2 w[16];
+                twiddles16<INV>(tw, k * step, w);
 #pragma unroll
-            for (int r = 1; r < R; ++r) {
-                float2 w = __ldg(tw + r * k * step);
-                if (INV) w.y = -w.y;
-                v[bi][r] = cmul(v[bi][r], w);
+                for (int r = 1; r < 16; ++r) v[bi][r] = cmul(v[bi][r], w[r]);
+            } else {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    float2 w = __ldg(tw + r * k * step);
+                    if (INV) w.y = -w.y;
+                    v[bi][r] = cmul(v[bi][r], w);
+                }
             }
         }
         dft<R, INV>(v[bi]);
@@ -200,8 +232,10 @@ __device__ __forceinline__ void fused_middle(float2* buf, int L, int tid, int T,
 #pragma unroll
         for (int r = 0; r < 16; ++r) v[bi][r] = buf[padi(j + r * LR)];
         if (LR > 1) {
+            float2 w[16];
+            twiddles16<false>(tw, j, w);
 #pragma unroll
-            for (int r = 1; r < 16; ++r) v[bi][r] = cmul(v[bi][r], __ldg(tw + r * j));
+            for (int r = 1; r < 16; ++r) v[bi][r] = cmul(v[bi][r], w[r]);
         }
         dft16<false>(v[bi]);
 #pragma unroll
@@ -218,7 +252,7 @@ __device__ __forceinline__ void fused_middle(float2* buf, int L, int tid, int T,
     __syncthreads();
 }
 
-// Filter one complex row pair in shared memory: forward FFT, Hs multiply,
+// Filter one complex row pair in shared memory: forward FFT, Hc multiply,
 // inverse FFT (natural order out). Radix-16 passes around the fused middle; the
 // radix-2/4/8 remainder pass runs first in the forward and last in the inverse.
 template <int K>

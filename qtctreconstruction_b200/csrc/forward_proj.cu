@@ -201,13 +201,10 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
                                                         const int* __restrict__ order,
                                                         float* __restrict__ sino,
                                                         unsigned* __restrict__ err) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float4* seg = reinterpret_cast<float4*>(smem_raw);  // [FNB][PCH][FW]
-    unsigned char* tail = smem_raw + sizeof(float4) * FNB * PCH * FW;
-    auto full = reinterpret_cast<unsigned long long*>(tail);
-    auto empty = full + FNB;
-    auto fa = reinterpret_cast<FAngle*>(tail + 16 * FNB);
-    auto qs_tab = reinterpret_cast<int*>(tail + 16 * FNB + sizeof(FAngle) * GMAX);
+    extern __shared__ __align__(128) float4 seg[];  // [FNB][PCH][FW] staged segments
+    __shared__ __align__(8) unsigned long long full[FNB], empty[FNB];
+    __shared__ FAngle fa[GMAX];
+    __shared__ int qs_tab[MAXCH];
 
     const int b0 = blockIdx.x * FB;
     const int b1 = min(b0 + FB, nd);  // exclusive
@@ -398,8 +395,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
                            int na, int nd, Trig trig, const int4* d_groups, int ngroups,
                            const int* d_order, float* d_sino, unsigned* d_err, cudaStream_t st) {
-    const size_t smem = sizeof(float4) * FNB * PCH * FW + 16 * FNB + sizeof(FAngle) * GMAX +
-                        sizeof(int) * MAXCH;
+    const size_t smem = sizeof(float4) * FNB * PCH * FW;
     const cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smem));
     if (e != cudaSuccess) return e;
