@@ -104,12 +104,13 @@ struct FAngle {
     int edge;  // an edge ray (bin 0 or nd-1) of this CTA reaches the image at this angle
 };
 
-// The fast path: tent weights of the (up to three) pixels around the crossing.
-// Loads are issued only where they can matter: rows where the crossing lies
-// outside the image (plus reach) and a third candidate with weight 0 are
-// predicated off, so they cost no shared-memory bandwidth.
+// The fast path: tent weights of the three pixels around the crossing. With
+// u0 = (qa - q*) |kq| in [-1, 0) for the first candidate qa = ceil(q* - R),
+// the weights 1 - |s - b| of the candidates qa, qa+1, qa+2 are 1 + u0,
+// 1 - |u0 + |kq||, and max(0, 1 - 2|kq| - u0) (the first two are never
+// negative, the third candidate is beyond reach when |kq| = 1).
 __device__ __forceinline__ void walk_chunk(const float4* __restrict__ sg, const FAngle& f, int t,
-                                           int p0, int qs, int nq, float4& acc) {
+                                           int p0, int qs, float4& acc) {
     const double qstar = fma(static_cast<double>(p0), f.dq, fma(static_cast<double>(t), f.inv, f.q0b0));
     const double qfl = floor(qstar);
     const float lq0 = static_cast<float>(static_cast<int>(qfl) - qs) + static_cast<float>(qstar - qfl);
@@ -118,31 +119,26 @@ __device__ __forceinline__ void walk_chunk(const float4* __restrict__ sg, const 
     // plane); never index outside the segment in that case.
     if (!(lq0 + fminf(0.0f, (PCH - 1) * f.dqf) >= 1.5f && lq0 + fmaxf(0.0f, (PCH - 1) * f.dqf) <= FW - 3.0f))
         return;
-    // image extent in segment coordinates, widened by the tent reach
-    const float lo_img = static_cast<float>(-qs) - f.R, hi_img = static_cast<float>(nq - 1 - qs) + f.R;
+    const float akq = fabsf(f.kqf);
+    const float c2 = 1.0f - 2.0f * akq;
 #pragma unroll
     for (int pp = 0; pp < PCH; ++pp) {
         const float qf = fmaf(static_cast<float>(pp), f.dqf, lq0);
-        if (qf < lo_img || qf > hi_img) continue;
         // first candidate ceil(qf - R), rounded by adding 1.5 * 2^23 (FADD and an
         // integer subtract instead of conversion-unit instructions); a tie moves
         // the three candidates by one pixel at distance exactly R (weight 0)
         const float tr = (qf + f.cr) + kRound;
         const int ia = __float_as_int(tr) - kRoundBits;
-        const float qa = tr - kRound;
-        const float t0 = (qa - qf) * f.kqf;  // s - b at candidate qa
+        const float u0 = ((tr - kRound) - qf) * akq;
+        const float w0 = 1.0f + u0;
+        const float w1 = 1.0f - fabsf(u0 + akq);
+        const float w2 = fmaxf(0.0f, c2 - u0);
         const float4* row = sg + pp * FW + ia;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float tt = fmaf(static_cast<float>(k), f.kqf, t0);
-            const float wgt = fmaxf(0.0f, 1.0f - fabsf(tt));
-            if (k == 2 && !(wgt > 0.0f)) break;
-            const float4 v = row[k];
-            acc.x = fmaf(wgt, v.x, acc.x);
-            acc.y = fmaf(wgt, v.y, acc.y);
-            acc.z = fmaf(wgt, v.z, acc.z);
-            acc.w = fmaf(wgt, v.w, acc.w);
-        }
+        const float4 v0 = row[0], v1 = row[1], v2 = row[2];
+        acc.x = fmaf(w2, v2.x, fmaf(w1, v1.x, fmaf(w0, v0.x, acc.x)));
+        acc.y = fmaf(w2, v2.y, fmaf(w1, v1.y, fmaf(w0, v0.y, acc.y)));
+        acc.z = fmaf(w2, v2.z, fmaf(w1, v1.z, fmaf(w0, v0.z, acc.z)));
+        acc.w = fmaf(w2, v2.w, fmaf(w1, v1.w, fmaf(w0, v0.w, acc.w)));
     }
 }
 
@@ -326,6 +322,23 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
                       FW * sizeof(float4), &full[buf]);
     };
 
+    // rows this warp's 32 rays can touch, per angle (warp-uniform): chunks
+    // outside them are skipped by the whole warp
+    int wlo_a = np, whi_a = -1, wlo_b = np, whi_b = -1;
+    {
+        const int wf = b0 + (tx & ~31), wl = min(wf + 31, nd - 1);
+        if (wf < nd) {
+            if (has_a) {
+                const FAngle& f = fa[ja];
+                prange(f.q0b0 + (wf - b0) * f.inv, f.q0b0 + (wl - b0) * f.inv, f.dq, fabs(f.inv) + 2.0, wlo_a, whi_a);
+            }
+            if (has_b) {
+                const FAngle& f = fa[jb];
+                prange(f.q0b0 + (wf - b0) * f.inv, f.q0b0 + (wl - b0) * f.inv, f.dq, fabs(f.inv) + 2.0, wlo_b, whi_b);
+            }
+        }
+    }
+
     // warps holding an edge ray that meets the image take the reference-decision path
     const int wb0 = b0 + (tx & ~31);
     const bool holds_edge = (wb0 <= 0 && 0 < wb0 + 32) || (wb0 <= nd - 1 && nd - 1 < wb0 + 32);
@@ -359,13 +372,13 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
         const int qs = qs_tab[ci];
         const float4* sg = seg + buf * PCH * FW;
         if (live) {
-            if (has_a) {
+            if (has_a && p0 <= whi_a && p0 + PCH - 1 >= wlo_a) {
                 if (edge_a) acc_a = walk_chunk_edge(sg, fa[ja], tx, p0, qs, b, nd, rows, cxf, cyf, acc_a);
-                else walk_chunk(sg, fa[ja], tx, p0, qs, nq, acc_a);
+                else walk_chunk(sg, fa[ja], tx, p0, qs, acc_a);
             }
-            if (has_b) {
+            if (has_b && p0 <= whi_b && p0 + PCH - 1 >= wlo_b) {
                 if (edge_b) acc_b = walk_chunk_edge(sg, fa[jb], tx, p0, qs, b, nd, rows, cxf, cyf, acc_b);
-                else walk_chunk(sg, fa[jb], tx, p0, qs, nq, acc_b);
+                else walk_chunk(sg, fa[jb], tx, p0, qs, acc_b);
             }
         }
         __syncwarp();
