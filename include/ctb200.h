@@ -165,6 +165,26 @@ ctb_status ctb_fbp_d(ctb_ctx* ctx, const float* d_sino, int depth, int num_angle
                      const float* angles_deg, int output_size, int filter, const float* d_stats,
                      int denorm, float* d_out);
 
+/* Ramp filtering + backprojection of 1..4 slices that allocates no device
+ * memory; it has no counterpart in the reference. It exists for callers that
+ * cannot allocate device memory where they reconstruct (a caller-owned memory
+ * pool, a real-time loop that must not wait on an allocator, a host whose
+ * allocator is not cudaMalloc) and so cannot create a context, whose
+ * workspaces are allocated on demand. The caller passes device buffers
+ * d_sino[depth][num_angles][bins] and d_out[depth][output_size]^2; the result
+ * is in normalised units, as ctb_fbp_d with d_stats = NULL, and the call
+ * returns after `stream` (a cudaStream_t, NULL = legacy default stream) has
+ * finished it. Every intermediate lives in one static 16 MiB device array that
+ * each GPU using the library keeps until the process exits: at most 2048
+ * angles, convolution length nextPow2(square_bins + bins - 1) <= 8192 and
+ * num_angles x (filtered row pitch) within the array; larger requests return
+ * CTB_ERR_UNSUPPORTED. The first call on a device looks up the array's device
+ * address (make it before any stream capture). All calls share the array, so
+ * calls that overlap on the GPU race. */
+ctb_status ctb_fbp_noalloc(const float* d_sino, int depth, int num_angles, int bins,
+                           const float* angles_deg, int output_size, int filter, float* d_out,
+                           void* stream);
+
 /* reconstructVolume on device buffers: forward + filter + backprojection +
  * Serial denormalisation. */
 ctb_status ctb_reconstruct_volume_d(ctb_ctx* ctx, const float* d_vol, int n, int depth,
