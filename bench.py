@@ -38,6 +38,8 @@ CONFIGS = {
                   name="128^3 phantom (10 ellipsoids), 180 angles, Ram-Lak"),
     "large": dict(n=512, nz=512, na=720, ellipsoids=32, filter=1, seed=2,
                   name="512^3 phantom (32 ellipsoids), 720 angles, Shepp-Logan"),
+    "medium": dict(n=384, nz=384, na=540, ellipsoids=24, filter=1, seed=4,
+                   name="384^3 phantom (24 ellipsoids), 540 angles, Shepp-Logan (profiling size)"),
     "precision": dict(n=1024, nz=256, na=1440, ellipsoids=64, filter=4, seed=3,
                       name="1024^2 x 256 phantom (64 ellipsoids), 1440 angles, Hann"),
 }

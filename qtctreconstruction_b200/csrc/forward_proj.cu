@@ -12,8 +12,7 @@
 //
 // A CTA owns FB = 128 consecutive bins, one group of up to GMAX = 8 angles that
 // share the walked image axis, and four slices (one float4 plane of the
-// normalised image). Thread (x, y) takes bin b0 + x for angles y and y + 4 of
-// the group. The ray family is walked along the image axis it is closest to
+// normalised image). Thread (x, y) takes bin b0 + x for angle y of the group. The ray family is walked along the image axis it is closest to
 // (rows when |cos| >= |sin|, else columns of the transposed copy), so every
 // step crosses at most three pixels of the gathered axis. Rows are processed
 // in chunks of PCH = 8; per chunk the row segments that any ray of any angle
@@ -41,9 +40,9 @@ constexpr int FB = kFwdRays;
 constexpr int PCH = kFwdRows;
 constexpr int FW = kFwdWidth;
 constexpr int GMAX = kFwdGroup;
-constexpr int AY = 4;            // angle lanes per CTA (each thread: angles y, y + AY)
+constexpr int AY = GMAX;         // angle lanes per CTA (thread (x, y): ray x, angle y)
 constexpr int THREADS = FB * AY;
-constexpr int FNB = 3;           // chunk buffers (pipeline depth)
+constexpr int FNB = 4;           // chunk buffers (pipeline depth)
 constexpr int MAXCH = 512;       // chunk table capacity (walked extent <= 4096)
 constexpr float kRound = 12582912.0f;  // 1.5 * 2^23: x + kRound rounds x to an integer
 constexpr int kRoundBits = 0x4B400000;  // bit pattern of kRound
@@ -190,7 +189,7 @@ __device__ __noinline__ float4 walk_chunk_edge(const float4* __restrict__ sg, co
     return acc;
 }
 
-__global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict__ img,
+__global__ void __launch_bounds__(THREADS, 1) k_forward(const float4* __restrict__ img,
                                                         const float4* __restrict__ imgT, int w,
                                                         int h, int nz, int na, int nd, Trig trig,
                                                         const int4* __restrict__ groups,
@@ -279,15 +278,14 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
         }
     }
     const bool live = b < nd;
-    const int ja = ty, jb = ty + AY;  // this thread's two angles of the group
-    const bool has_a = ja < cnt, has_b = jb < cnt;
+    const int ja = ty;  // this thread's angle of the group
+    const bool has_a = ja < cnt;
     if (p_hi < p_lo) {  // no ray of this CTA meets the image
         if (live)
             for (int k = 0; k < 4; ++k) {
                 const int z = 4 * g + k;
                 if (z >= nz) break;
                 if (has_a) sino[(static_cast<long long>(z) * na + fa[ja].a) * nd + b] = 0.0f;
-                if (has_b) sino[(static_cast<long long>(z) * na + fa[jb].a) * nd + b] = 0.0f;
             }
         return;
     }
@@ -324,18 +322,12 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
 
     // rows this warp's 32 rays can touch, per angle (warp-uniform): chunks
     // outside them are skipped by the whole warp
-    int wlo_a = np, whi_a = -1, wlo_b = np, whi_b = -1;
+    int wlo_a = np, whi_a = -1;
     {
         const int wf = b0 + (tx & ~31), wl = min(wf + 31, nd - 1);
-        if (wf < nd) {
-            if (has_a) {
-                const FAngle& f = fa[ja];
-                prange(f.q0b0 + (wf - b0) * f.inv, f.q0b0 + (wl - b0) * f.inv, f.dq, fabs(f.inv) + 2.0, wlo_a, whi_a);
-            }
-            if (has_b) {
-                const FAngle& f = fa[jb];
-                prange(f.q0b0 + (wf - b0) * f.inv, f.q0b0 + (wl - b0) * f.inv, f.dq, fabs(f.inv) + 2.0, wlo_b, whi_b);
-            }
+        if (wf < nd && has_a) {
+            const FAngle& f = fa[ja];
+            prange(f.q0b0 + (wf - b0) * f.inv, f.q0b0 + (wl - b0) * f.inv, f.dq, fabs(f.inv) + 2.0, wlo_a, whi_a);
         }
     }
 
@@ -343,10 +335,9 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     const int wb0 = b0 + (tx & ~31);
     const bool holds_edge = (wb0 <= 0 && 0 < wb0 + 32) || (wb0 <= nd - 1 && nd - 1 < wb0 + 32);
     const bool edge_a = holds_edge && has_a && fa[ja].edge;
-    const bool edge_b = holds_edge && has_b && fa[jb].edge;
     const float cxf = static_cast<float>(w - 1) * 0.5f, cyf = static_cast<float>(h - 1) * 0.5f;
 
-    float4 acc_a = make_float4(0.f, 0.f, 0.f, 0.f), acc_b = acc_a;
+    float4 acc_a = make_float4(0.f, 0.f, 0.f, 0.f);
     int last_issued = -1;  // producer only
     if (tid == 0)
         for (int ci = 0; ci < FNB - 1 && ci < nch; ++ci) {
@@ -376,10 +367,6 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
                 if (edge_a) acc_a = walk_chunk_edge(sg, fa[ja], tx, p0, qs, b, nd, rows, cxf, cyf, acc_a);
                 else walk_chunk(sg, fa[ja], tx, p0, qs, acc_a);
             }
-            if (has_b && p0 <= whi_b && p0 + PCH - 1 >= wlo_b) {
-                if (edge_b) acc_b = walk_chunk_edge(sg, fa[jb], tx, p0, qs, b, nd, rows, cxf, cyf, acc_b);
-                else walk_chunk(sg, fa[jb], tx, p0, qs, acc_b);
-            }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[buf]);
@@ -393,13 +380,11 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     }
     if (!live) return;
     const float ra[4] = {acc_a.x, acc_a.y, acc_a.z, acc_a.w};
-    const float rb[4] = {acc_b.x, acc_b.y, acc_b.z, acc_b.w};
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int z = 4 * g + k;
         if (z >= nz) break;
         if (has_a) sino[(static_cast<long long>(z) * na + fa[ja].a) * nd + b] = ra[k];
-        if (has_b) sino[(static_cast<long long>(z) * na + fa[jb].a) * nd + b] = rb[k];
     }
 }
 
