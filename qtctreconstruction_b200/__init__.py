@@ -24,7 +24,8 @@ from typing import Callable, Optional
 import numpy as np
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "libctb200.so")
+# CTB200_LIB selects another build of the library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("CTB200_LIB", os.path.join(PKG, "libctb200.so"))
 
 
 class FilterType(enum.IntEnum):

@@ -78,7 +78,7 @@ cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const flo
 constexpr int kFwdRays = 128;   // rays (detector bins) per CTA
 constexpr int kFwdRows = 8;     // walked rows per staged chunk
 constexpr int kFwdWidth = 256;  // staged pixels per row
-constexpr int kFwdGroup = 8;    // angles per CTA
+constexpr int kFwdGroup = 4;    // angles per CTA
 // Zero border of the normalised image planes: kFwdGuard pixels on both sides
 // of every row (>= kFwdWidth + reach) and kFwdRows rows after the last, so a
 // staged segment never leaves the plane.

@@ -10,17 +10,17 @@
 // weight 1 - |s - b| (the identical weights (1-frac, frac) of the splat).
 // Sinogram stores are coalesced by detector bin.
 //
-// A CTA owns FB = 128 consecutive bins, one group of up to GMAX = 8 angles that
+// A CTA owns FB = 128 consecutive bins, one group of up to GMAX = 4 angles that
 // share the walked image axis, and four slices (one float4 plane of the
 // normalised image). Thread (x, y) takes bin b0 + x for angle y of the group. The ray family is walked along the image axis it is closest to
 // (rows when |cos| >= |sin|, else columns of the transposed copy), so every
 // step crosses at most three pixels of the gathered axis. Rows are processed
 // in chunks of PCH = 8; per chunk the row segments that any ray of any angle
 // of the CTA can touch (FW pixels per row) are staged once into shared memory
-// by the bulk-copy engine and read by all eight angles. The image planes carry
+// by the bulk-copy engine and read by all angles of the group. The image planes carry
 // a zero border (kFwdGuard), so a segment never needs filling. Staging is a
 // producer/consumer pipeline: two buffers, each with a "full" mbarrier (bytes
-// landed) and an "empty" mbarrier (all 16 warps done), so warps never wait on
+// landed) and an "empty" mbarrier (all warps done), so warps never wait on
 // one another at a CTA-wide barrier. The host forms the
 // groups so that the segment width provably fits (forward_plan). The crossing
 // point q*(b, p) is evaluated in double once per chunk and angle and split
@@ -42,7 +42,7 @@ constexpr int FW = kFwdWidth;
 constexpr int GMAX = kFwdGroup;
 constexpr int AY = GMAX;         // angle lanes per CTA (thread (x, y): ray x, angle y)
 constexpr int THREADS = FB * AY;
-constexpr int FNB = 4;           // chunk buffers (pipeline depth)
+constexpr int FNB = 3;           // chunk buffers (pipeline depth)
 constexpr int MAXCH = 512;       // chunk table capacity (walked extent <= 4096)
 constexpr float kRound = 12582912.0f;  // 1.5 * 2^23: x + kRound rounds x to an integer
 constexpr int kRoundBits = 0x4B400000;  // bit pattern of kRound
@@ -133,7 +133,9 @@ __device__ __forceinline__ void walk_chunk(const float4* __restrict__ sg, const 
         const float w1 = 1.0f - fabsf(u0 + akq);
         const float w2 = fmaxf(0.0f, c2 - u0);
         const float4* row = sg + pp * FW + ia;
-        const float4 v0 = row[0], v1 = row[1], v2 = row[2];
+        const float4 v0 = row[0], v1 = row[1];
+        // the third candidate is loaded only where it carries weight
+        const float4 v2 = w2 > 0.0f ? row[2] : make_float4(0.f, 0.f, 0.f, 0.f);
         acc.x = fmaf(w2, v2.x, fmaf(w1, v1.x, fmaf(w0, v0.x, acc.x)));
         acc.y = fmaf(w2, v2.y, fmaf(w1, v1.y, fmaf(w0, v0.y, acc.y)));
         acc.z = fmaf(w2, v2.z, fmaf(w1, v1.z, fmaf(w0, v0.z, acc.z)));
@@ -189,7 +191,7 @@ __device__ __noinline__ float4 walk_chunk_edge(const float4* __restrict__ sg, co
     return acc;
 }
 
-__global__ void __launch_bounds__(THREADS, 1) k_forward(const float4* __restrict__ img,
+__global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict__ img,
                                                         const float4* __restrict__ imgT, int w,
                                                         int h, int nz, int na, int nd, Trig trig,
                                                         const int4* __restrict__ groups,
