@@ -259,18 +259,11 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     Trig trig;
     CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
     CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream));
-    // occupancy bitmaps (rows include the kFwdRows border rows, which stay clear)
-    const size_t occ_n = static_cast<size_t>(nzg) * (h + kFwdRows) * occ_words(w);
-    const size_t occT_n = static_cast<size_t>(nzg) * (w + kFwdRows) * occ_words(h);
-    CTB_WS(ctx, d_occ, unsigned, "occ", occ_n);
-    CTB_WS(ctx, d_occT, unsigned, "occT", occT_n);
-    CTB_CUDA(ctx, cudaMemsetAsync(d_occ, 0, sizeof(unsigned) * occ_n, ctx->stream));
-    CTB_CUDA(ctx, cudaMemsetAsync(d_occT, 0, sizeof(unsigned) * occT_n, ctx->stream));
-    CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, d_occ, d_occT, ctx->stream));
+    CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream));
     mark(ctx, ev, 1);
     const ctb_ctx::FwdPlanDev* plan = nullptr;
     CTB_TRY(forward_plan_dev(ctx, angles_deg, na, w, h, nd, &plan));
-    CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, d_occ, d_occT, w, h, nz, na, nd, trig,
+    CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd, trig,
                                    static_cast<const int4*>(plan->groups.ptr), plan->ngroups,
                                    static_cast<const int*>(plan->order.ptr), d_sino, ctx->d_err,
                                    ctx->stream));

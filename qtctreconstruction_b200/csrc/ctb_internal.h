@@ -11,12 +11,6 @@
 
 #include "../../include/ctb200.h"
 
-#ifdef __CUDACC__
-#define CTB_HD __host__ __device__
-#else
-#define CTB_HD
-#endif
-
 namespace ctb {
 
 // ----------------------------------------------------------------- geometry
@@ -75,16 +69,8 @@ struct Trig {
 cudaError_t launch_trig(const float* d_angles_deg, int na, double2* d_cs, cudaStream_t st);
 cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4* d_stats,
                                cudaStream_t st);
-// Occupancy of the normalised planes: one bit per kOccSeg-pixel segment of a
-// plane row (set when any of the 4 slices is non-zero there), occ_words(nq)
-// 32-bit words per row; occ for the row-walked plane, occT for the
-// column-walked one. The projector skips row segments whose bits are clear:
-// the reference skips zero pixels (SerialBackend.cpp:104).
-constexpr int kOccSeg = 32;
-CTB_HD inline int occ_words(int nq) { return ((nq + kOccSeg - 1) / kOccSeg + 31) / 32 + 1; }
 cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
-                             float4* d_img, float4* d_imgT, unsigned* d_occ, unsigned* d_occT,
-                             cudaStream_t st);
+                             float4* d_img, float4* d_imgT, cudaStream_t st);
 // Forward projector work plan: angles grouped (up to kFwdGroup per CTA) by
 // walked axis so that one staged row segment of kFwdWidth pixels serves every
 // angle of the group. groups: {first index into order, count, axis (0 rows,
@@ -105,10 +91,9 @@ struct FwdPlan {
     std::vector<int> groups;  // 4 ints per group
 };
 FwdPlan forward_plan(const float* angles_deg, int na, int w, int h, int nd);
-cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, const unsigned* d_occ,
-                           const unsigned* d_occT, int w, int h, int nz, int na, int nd, Trig trig,
-                           const int4* d_groups, int ngroups, const int* d_order, float* d_sino,
-                           unsigned* d_err, cudaStream_t st);
+cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
+                           int na, int nd, Trig trig, const int4* d_groups, int ngroups,
+                           const int* d_order, float* d_sino, unsigned* d_err, cudaStream_t st);
 cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
                           const FiltLayout& fl, const float2* d_Hc, const float2* d_tw,
                           const float4* d_stats, int denorm, float scale, float4* d_filt,

@@ -73,10 +73,7 @@ __global__ void __launch_bounds__(1024) k_slice_stats(const float* __restrict__ 
 // written here, the borders are zeroed when the buffers are set up.
 __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol, int w, int h, int nz,
                                                    const float4* __restrict__ stats,
-                                                   float4* __restrict__ img, float4* __restrict__ imgT,
-                                                   unsigned* __restrict__ occ,
-                                                   unsigned* __restrict__ occT) {
-    const int ow = occ_words(w), owT = occ_words(h);
+                                                   float4* __restrict__ img, float4* __restrict__ imgT) {
     const long long pw = w + 2 * kFwdGuard, ph = h + 2 * kFwdGuard;  // row pitches
     const long long rw = h + kFwdRows, rh = w + kFwdRows;             // rows per plane
     __shared__ float4 tile[32][33];
@@ -108,24 +105,12 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
         const float4 q = make_float4(v[0], v[1], v[2], v[3]);
         tile[ty + 8 * r][tx] = q;
         if (x < w && y < h) img[(zg * rw + y) * pw + x + kFwdGuard] = q;
-        // occupancy bit of row y, segment x0/32 (the tile's 32 columns)
-        const bool nz_px = v[0] != 0.0f || v[1] != 0.0f || v[2] != 0.0f || v[3] != 0.0f;
-        if (__ballot_sync(0xffffffffu, nz_px) && tx == 0 && y < h) {
-            const int sgm = x0 / kOccSeg;
-            atomicOr(occ + (zg * rw + y) * ow + sgm / 32, 1u << (sgm % 32));
-        }
     }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int x = x0 + ty + 8 * r, y = y0 + tx;
-        const float4 q = tile[tx][ty + 8 * r];
-        if (x < w && y < h) imgT[(zg * rh + x) * ph + y + kFwdGuard] = q;
-        const bool nz_px = q.x != 0.0f || q.y != 0.0f || q.z != 0.0f || q.w != 0.0f;
-        if (__ballot_sync(0xffffffffu, nz_px) && tx == 0 && x < w) {
-            const int sgm = y0 / kOccSeg;
-            atomicOr(occT + (zg * rh + x) * owT + sgm / 32, 1u << (sgm % 32));
-        }
+        if (x < w && y < h) imgT[(zg * rh + x) * ph + y + kFwdGuard] = tile[tx][ty + 8 * r];
     }
 }
 
@@ -143,10 +128,9 @@ cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4
 }
 
 cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
-                             float4* d_img, float4* d_imgT, unsigned* d_occ, unsigned* d_occT,
-                             cudaStream_t st) {
+                             float4* d_img, float4* d_imgT, cudaStream_t st) {
     const dim3 grid((w + 31) / 32, (h + 31) / 32, (nz + 3) / 4);
-    k_normalize<<<grid, 256, 0, st>>>(d_vol, w, h, nz, d_stats, d_img, d_imgT, d_occ, d_occT);
+    k_normalize<<<grid, 256, 0, st>>>(d_vol, w, h, nz, d_stats, d_img, d_imgT);
     return cudaGetLastError();
 }
 

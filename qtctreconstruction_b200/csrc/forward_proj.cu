@@ -109,39 +109,19 @@ struct FAngle {
 // 1 - |u0 + |kq||, and max(0, 1 - 2|kq| - u0) (the first two are never
 // negative, the third candidate is beyond reach when |kq| = 1).
 __device__ __forceinline__ void walk_chunk(const float4* __restrict__ sg, const FAngle& f, int t,
-                                           int p0, int qs, int nq, const unsigned* __restrict__ occ,
-                                           int ow, float4& acc) {
+                                           int p0, int qs, float4& acc) {
     const double qstar = fma(static_cast<double>(p0), f.dq, fma(static_cast<double>(t), f.inv, f.q0b0));
     const double qfl = floor(qstar);
     const float lq0 = static_cast<float>(static_cast<int>(qfl) - qs) + static_cast<float>(qstar - qfl);
     // Every crossing of every ray of the CTA lies in [3, FW - 6] of the segment
     // unless the chunk meets no ray at all (segment start clamped to the
-    // plane); such lanes never index outside the segment. Called by whole
-    // warps (the shuffles below), so the guard is a predicate, not a return.
-    const bool in_seg = lq0 + fminf(0.0f, (PCH - 1) * f.dqf) >= 1.5f &&
-                        lq0 + fmaxf(0.0f, (PCH - 1) * f.dqf) <= FW - 3.0f;
+    // plane); never index outside the segment in that case.
+    if (!(lq0 + fminf(0.0f, (PCH - 1) * f.dqf) >= 1.5f && lq0 + fmaxf(0.0f, (PCH - 1) * f.dqf) <= FW - 3.0f))
+        return;
     const float akq = fabsf(f.kqf);
     const float c2 = 1.0f - 2.0f * akq;
-    // the warp's crossings span [qw_lo, qw_hi] at p0 (they are monotone in the lane)
-    const float qa_l0 = __shfl_sync(0xffffffffu, lq0, 0), qa_l31 = __shfl_sync(0xffffffffu, lq0, 31);
-    const float qw_lo = fminf(qa_l0, qa_l31) - f.R - 1.0f, qw_hi = fmaxf(qa_l0, qa_l31) + f.R + 2.0f;
-    if (!in_seg) return;
 #pragma unroll
     for (int pp = 0; pp < PCH; ++pp) {
-        // skip rows whose touched segments hold only zero pixels (warp-uniform:
-        // every lane computes the same range)
-        {
-            const int lo = max(0, qs + static_cast<int>(floorf(qw_lo + pp * f.dqf)));
-            const int hi = min(nq - 1, qs + static_cast<int>(ceilf(qw_hi + pp * f.dqf)));
-            if (hi < lo) continue;
-            const int s0 = lo / kOccSeg, s1 = hi / kOccSeg, w0 = s0 >> 5;
-            const int b0 = s0 - 32 * w0, nb = s1 - s0 + 1;
-            if (nb <= 32) {
-                const unsigned* o = occ + static_cast<long long>(p0 + pp) * ow + w0;
-                const unsigned long long bits = (static_cast<unsigned long long>(__ldg(o + 1)) << 32) | __ldg(o);
-                if (((bits >> b0) & ((1ull << nb) - 1ull)) == 0ull) continue;
-            }
-        }
         const float qf = fmaf(static_cast<float>(pp), f.dqf, lq0);
         // first candidate ceil(qf - R), rounded by adding 1.5 * 2^23 (FADD and an
         // integer subtract instead of conversion-unit instructions); a tie moves
@@ -212,9 +192,7 @@ __device__ __noinline__ float4 walk_chunk_edge(const float4* __restrict__ sg, co
 }
 
 __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict__ img,
-                                                        const float4* __restrict__ imgT,
-                                                        const unsigned* __restrict__ occ_rows,
-                                                        const unsigned* __restrict__ occ_cols, int w,
+                                                        const float4* __restrict__ imgT, int w,
                                                         int h, int nz, int na, int nd, Trig trig,
                                                         const int4* __restrict__ groups,
                                                         const int* __restrict__ order,
@@ -331,8 +309,6 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     __syncthreads();
 
     const long long pitch = nq + 2 * kFwdGuard;
-    const int ow = occ_words(nq);
-    const unsigned* occ = (rows ? occ_rows : occ_cols) + static_cast<long long>(g) * (np + PCH) * ow;
     const float4* plane = (rows ? img : imgT) + static_cast<long long>(g) * (np + PCH) * pitch + kFwdGuard;
 
     // producer (thread 0): stage chunk ci into buffer buf; rows p0..p0+7 exist
@@ -388,13 +364,10 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
         const int p0 = p_lo + ci * PCH;
         const int qs = qs_tab[ci];
         const float4* sg = seg + buf * PCH * FW;
-        // warp-uniform: has_a, the warp's row range and edge_a are per warp; lanes
-        // past the last bin walk harmlessly and never store
-        if (has_a && p0 <= whi_a && p0 + PCH - 1 >= wlo_a) {
-            if (edge_a) {
-                if (live) acc_a = walk_chunk_edge(sg, fa[ja], tx, p0, qs, b, nd, rows, cxf, cyf, acc_a);
-            } else {
-                walk_chunk(sg, fa[ja], tx, p0, qs, nq, occ, ow, acc_a);
+        if (live) {
+            if (has_a && p0 <= whi_a && p0 + PCH - 1 >= wlo_a) {
+                if (edge_a) acc_a = walk_chunk_edge(sg, fa[ja], tx, p0, qs, b, nd, rows, cxf, cyf, acc_a);
+                else walk_chunk(sg, fa[ja], tx, p0, qs, acc_a);
             }
         }
         __syncwarp();
@@ -419,10 +392,9 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
 
 }  // namespace
 
-cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, const unsigned* d_occ,
-                           const unsigned* d_occT, int w, int h, int nz, int na, int nd, Trig trig,
-                           const int4* d_groups, int ngroups, const int* d_order, float* d_sino,
-                           unsigned* d_err, cudaStream_t st) {
+cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
+                           int na, int nd, Trig trig, const int4* d_groups, int ngroups,
+                           const int* d_order, float* d_sino, unsigned* d_err, cudaStream_t st) {
     const size_t smem = sizeof(float4) * FNB * PCH * FW;
     const cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smem));
@@ -430,8 +402,8 @@ cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, const unsi
     const int np = w > h ? w : h;
     if ((np + PCH - 1) / PCH + 1 > MAXCH) return cudaErrorInvalidValue;
     const dim3 grid((nd + FB - 1) / FB, ngroups, (nz + 3) / 4);
-    k_forward<<<grid, dim3(FB, AY), smem, st>>>(d_img, d_imgT, d_occ, d_occT, w, h, nz, na, nd, trig,
-                                                d_groups, d_order, d_sino, d_err);
+    k_forward<<<grid, dim3(FB, AY), smem, st>>>(d_img, d_imgT, w, h, nz, na, nd, trig, d_groups,
+                                                d_order, d_sino, d_err);
     return cudaGetLastError();
 }
 
