@@ -134,8 +134,8 @@ def gpu_id_for(device: int) -> str:
 
 
 def load_profile_traffic(config: str):
-    """DRAM bytes per backprojection launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", f"backproject_{config}_traffic.json")
+    """DRAM bytes per backprojection launch from the committed ncu summary (JSON text), if any."""
+    path = os.path.join(ROOT, "profiles", f"backproject_{config}_traffic.txt")
     try:
         with open(path) as f:
             return json.load(f).get("dram_bytes_per_launch")
