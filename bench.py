@@ -11,7 +11,7 @@ data (no dataset involved); the volume (0.54 GB) exceeds the 126 MB L2, so no
 flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config small|large|precision]
+                  [--config small|large|medium|precision|batch]
 
 N > 1 runs under torch.distributed.run, one rank per GPU, each rank
 reconstructing its own volume (weak scaling; no data-path collective).
@@ -42,6 +42,9 @@ CONFIGS = {
                    name="384^3 phantom (24 ellipsoids), 540 angles, Shepp-Logan (profiling size)"),
     "precision": dict(n=1024, nz=256, na=1440, ellipsoids=64, filter=4, seed=3,
                       name="1024^2 x 256 phantom (64 ellipsoids), 1440 angles, Hann"),
+    "batch": dict(jobs=64, seed=4,
+                  name="64 uneven FBP jobs: N in {64..768}, 16-256 slices, round(pi/2 N) angles, "
+                       "Ram-Lak/Shepp-Logan/Hann, sinograms of seeded 10-ellipsoid phantoms"),
 }
 FILTER_NAMES = ["ramlak", "shepp-logan", "hamming", "cosine", "hann", "bartlett"]
 METRIC = "FBP voxel-angle updates/s"
@@ -359,6 +362,103 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
     return 0
 
 
+# ------------------------------------------------------------------ batches
+BATCH_FILTERS = (0, 1, 4)  # Ram-Lak, Shepp-Logan, Hann
+
+
+def batch_shapes(seed: int, count: int):
+    """The uneven job mix: N uniform in {64, 96, ..., 768}, slices uniform in
+    [16, 256], angles round(pi/2 N), Nd odd >= sqrt(2) N, filter uniform over
+    Ram-Lak / Shepp-Logan / Hann."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.choice(np.arange(64, 769, 32)))
+        out.append(dict(n=n, nz=int(rng.integers(16, 257)), na=int(round(math.pi / 2 * n)), nd=odd_nd(n),
+                        filter=int(rng.choice(BATCH_FILTERS))))
+    return out
+
+
+def make_batch_inputs(be, torch, shapes, seed: int):
+    """Device sinograms of seeded random-ellipsoid phantoms (forward-projected
+    on the GPU) and output buffers for every job."""
+    import qtctreconstruction_b200 as ctb
+    jobs, keep = [], []
+    for k, s in enumerate(shapes):
+        n, nz, na, nd = s["n"], s["nz"], s["na"], s["nd"]
+        vol = torch.empty((nz, n, n), dtype=torch.float32, device="cuda")
+        be.phantom_d(ctb.phantom_params(seed * 1000 + k, 10), n, n, nz, vol.data_ptr())
+        sino = torch.empty((nz, na, nd), dtype=torch.float32, device="cuda")
+        stats = torch.empty((nz, 4), dtype=torch.float32, device="cuda")
+        be.forward_d(vol.data_ptr(), n, nz, na, nd, sino.data_ptr(), stats.data_ptr())
+        be.synchronize()
+        del vol
+        out = torch.empty((nz, n, n), dtype=torch.float32, device="cuda")
+        keep.append((sino, out))
+        jobs.append(dict(sino=sino.data_ptr(), depth=nz, num_angles=na, bins=nd, output_size=n,
+                         filter=s["filter"], out=out.data_ptr()))
+    return jobs, keep
+
+
+def run_batch(args, cfg, rank: int, world: int, local: int):
+    """Config "batch": `jobs` uneven FBP jobs from device-resident sinograms.
+    One step = every job filtered and backprojected. Timed three ways on the
+    same jobs: the batch replayed from a CUDA graph (the value), the batch
+    launched directly, and one filter + one backprojection launch per job."""
+    import torch
+
+    import qtctreconstruction_b200 as ctb
+    torch.cuda.set_device(local)
+    be = ctb.B200Backend(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    be.set_stream(stream.cuda_stream)
+    shapes = batch_shapes(cfg["seed"], cfg["jobs"])
+    jobs, keep = make_batch_inputs(be, torch, shapes, cfg["seed"])
+    updates = sum(s["n"] ** 2 * s["nz"] * s["na"] for s in shapes)
+    results, outputs = {}, {}
+    for mode, flags in (("graph", ctb.BATCH_GRAPH), ("direct", 0), ("per_job", ctb.BATCH_PER_JOB)):
+        with be.batch(jobs, flags) as b:
+            launches, _, nbytes = b.info()
+            for _ in range(args.warmup):
+                b.run()
+            torch.cuda.synchronize()
+            sampler = ClockSampler(gpu_id_for(local)) if mode == "graph" else None
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                b.run()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            be.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            results[mode] = dict(ms_per_step=ms, value=updates / (ms * 1e-3), launches_per_step=launches,
+                                 device_bytes=nbytes)
+            if sampler:
+                results[mode]["clocks"] = sampler.stop()
+            outputs[mode] = [o.sum().item() for _, o in keep[:4]]
+    same = outputs["graph"] == outputs["direct"] == outputs["per_job"]
+    g = results["graph"]
+    line = {
+        "metric": METRIC, "value": g["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": g["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batch", "description": cfg["name"], "jobs": len(shapes),
+                   "voxels": sum(s["n"] ** 2 * s["nz"] for s in shapes),
+                   "sinogram_bytes": sum(4 * s["nz"] * s["na"] * s["nd"] for s in shapes),
+                   "l2": "inputs larger than L2, no flush"},
+        "gpu_launches": g["launches_per_step"] * args.steps,
+        "modes": results,
+        "batched_vs_per_job": results["per_job"]["ms_per_step"] / g["ms_per_step"],
+        "outputs_identical_across_modes": same,
+        "clocks": g.get("clocks"),
+    }
+    print(json.dumps(line), flush=True)
+    be.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -375,6 +475,11 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     cfg = CONFIGS[args.config]
+    if args.config == "batch":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batch entry point"}))
+            return 0
+        return run_batch(args, cfg, rank, world, local) if rank == 0 else 0
     if args.impl == "reference":
         return run_reference(args, cfg, rank, world)
     return run_ours(args, cfg, rank, world, local)

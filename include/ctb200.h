@@ -190,6 +190,52 @@ ctb_status ctb_fbp_noalloc(const float* d_sino, int depth, int num_angles, int b
 ctb_status ctb_reconstruct_volume_d(ctb_ctx* ctx, const float* d_vol, int n, int depth,
                                     int num_angles, int detector_bins, int filter, float* d_out);
 
+/* ------------------------------------------------------------ batches */
+
+/* One FBP job of a batch: ramp filtering + backprojection of device sinograms
+ * sino[depth][num_angles][bins] into out[depth][output_size]^2, in normalised
+ * units (ctb_fbp_d with d_stats = NULL). angles_deg is a host array read when
+ * the batch is created (NULL = uniform 180/na * a). No counterpart in the
+ * reference, which reconstructs one volume per call
+ * (IReconstructionBackend.h:39-44); a job's result is bit-identical to
+ * ctb_fbp_d on the same job and does not depend on the other jobs. */
+typedef struct ctb_fbp_job {
+    const float* sino;
+    int depth;
+    int num_angles;
+    int bins;
+    const float* angles_deg;
+    int output_size;
+    int filter;
+    float* out;
+} ctb_fbp_job;
+
+typedef struct ctb_batch ctb_batch;
+
+enum {
+    CTB_BATCH_GRAPH = 1,    /* capture the launches once as a CUDA graph; ctb_batch_run replays it */
+    CTB_BATCH_PER_JOB = 2   /* one filter + one backprojection launch per job (comparison mode) */
+};
+
+/* Plan a batch: device state for every job (angle tables, filtered rows) is
+ * allocated here, jobs are grouped by convolution length, and the work of all
+ * jobs shares one filter launch per length class and one persistent
+ * backprojection launch (a work queue of (job, slice group, tile) items,
+ * longest jobs first). The batch keeps the job pointers; it must be destroyed
+ * before its context. */
+ctb_status ctb_batch_create(ctb_ctx* ctx, const ctb_fbp_job* jobs, int njobs, int flags,
+                            ctb_batch** out);
+/* Enqueue the batch on the context's stream (asynchronous). */
+ctb_status ctb_batch_run(ctb_batch* batch);
+/* Kernel launches (or graph launches) one ctb_batch_run issues; voxel-angle
+ * updates of the whole batch (sum of output_size^2 * depth * num_angles). */
+ctb_status ctb_batch_info(const ctb_batch* batch, int* launches, double* updates,
+                          size_t* device_bytes);
+void ctb_batch_destroy(ctb_batch* batch);
+
+/* ctb_batch_create + run + synchronise + destroy. */
+ctb_status ctb_fbp_batch_d(ctb_ctx* ctx, const ctb_fbp_job* jobs, int njobs);
+
 /* ------------------------------------------------------------ phantoms */
 
 /* Summed random-ellipsoid phantom (the benchmark phantom; a new generator mode

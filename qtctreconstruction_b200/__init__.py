@@ -73,6 +73,17 @@ _lib = None
 _F32P = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 
 
+class FbpJob(ctypes.Structure):
+    """ctb_fbp_job: one job of a batch (device pointers, host angle list or None)."""
+    _fields_ = [("sino", ctypes.c_void_p), ("depth", ctypes.c_int), ("num_angles", ctypes.c_int),
+                ("bins", ctypes.c_int), ("angles_deg", ctypes.c_void_p), ("output_size", ctypes.c_int),
+                ("filter", ctypes.c_int), ("out", ctypes.c_void_p)]
+
+
+BATCH_GRAPH = 1    # CTB_BATCH_GRAPH
+BATCH_PER_JOB = 2  # CTB_BATCH_PER_JOB
+
+
 def library() -> ctypes.CDLL:
     """Load libctb200.so (raises if it was never built)."""
     global _lib
@@ -120,6 +131,12 @@ def _declare(L):
     L.ctb_set_profiling.argtypes = [p, i]
     L.ctb_stage_times.argtypes = [p, i, P(ctypes.c_double)]
     L.ctb_probe_smem_bandwidth.argtypes = [p, P(ctypes.c_double)]
+    L.ctb_batch_create.argtypes = [p, P(FbpJob), i, i, P(p)]
+    L.ctb_batch_run.argtypes = [p]
+    L.ctb_batch_info.argtypes = [p, P(i), P(ctypes.c_double), P(ctypes.c_size_t)]
+    L.ctb_batch_destroy.argtypes = [p]
+    L.ctb_batch_destroy.restype = None
+    L.ctb_fbp_batch_d.argtypes = [p, P(FbpJob), i]
 
 
 # ----------------------------------------------------------------- helpers
@@ -377,10 +394,75 @@ class B200Backend:
         self._check(self._lib.ctb_reconstruct_volume_d(self._h, ctypes.c_void_p(d_vol), n, depth, na, nd,
                                                        int(kind), ctypes.c_void_p(d_out)), "reconstruct_volume_d")
 
+    def _jobs(self, jobs):
+        """ctypes array of FbpJob from dicts {sino, depth, num_angles, bins, output_size, filter,
+        out[, angles_deg]} (device pointers as ints); keeps angle arrays alive on the array."""
+        arr = (FbpJob * len(jobs))()
+        keep = []
+        for k, j in enumerate(jobs):
+            ang = j.get("angles_deg")
+            ap = None
+            if ang is not None:
+                a = _f32(ang)
+                keep.append(a)
+                ap = a.ctypes.data
+            arr[k] = FbpJob(j["sino"], j["depth"], j["num_angles"], j["bins"], ap, j["output_size"],
+                            int(j["filter"]), j["out"])
+        arr._keep = keep
+        return arr
+
+    def fbp_batch_d(self, jobs):
+        """Filter + backproject many device jobs in one batch (ctb_fbp_batch_d); synchronous."""
+        arr = self._jobs(jobs)
+        self._check(self._lib.ctb_fbp_batch_d(self._h, arr, len(jobs)), "fbp_batch_d")
+
+    def batch(self, jobs, flags: int = 0) -> "Batch":
+        return Batch(self, jobs, flags)
+
     def phantom_d(self, params: np.ndarray, nx: int, ny: int, nz: int, d_vol: int):
         p = _f32(params).reshape(-1)
         self._check(self._lib.ctb_phantom_sum_d(self._h, p, p.size // 16, nx, ny, nz, ctypes.c_void_p(d_vol)),
                     "phantom_d")
+
+
+class Batch:
+    """A planned batch (ctb_batch_create); run() enqueues it on the backend's stream."""
+
+    def __init__(self, backend: B200Backend, jobs, flags: int = 0):
+        self._be = backend
+        self._lib = backend._lib
+        arr = backend._jobs(jobs)
+        h = ctypes.c_void_p()
+        backend._check(self._lib.ctb_batch_create(backend.handle, arr, len(jobs), int(flags), ctypes.byref(h)),
+                       "batch_create")
+        self._h = h
+
+    def run(self):
+        self._be._check(self._lib.ctb_batch_run(self._h), "batch_run")
+
+    def info(self):
+        """(kernel launches per run, voxel-angle updates, device bytes)."""
+        n, u, b = ctypes.c_int(), ctypes.c_double(), ctypes.c_size_t()
+        self._be._check(self._lib.ctb_batch_info(self._h, ctypes.byref(n), ctypes.byref(u), ctypes.byref(b)),
+                        "batch_info")
+        return n.value, u.value, b.value
+
+    def close(self):
+        if self._h:
+            self._lib.ctb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 # Generator3D::Params defaults (Generator3D.h:16-34): soft tissue, then bone.
@@ -388,6 +470,6 @@ GENERATOR3D_TISSUE = np.array(
     [-20.0, 45.0, 3.0, 10.0, 0.0, 0.0, 0.0, 1.0,
      200.0, 1000.0, 2.0, 8.0, 1.0, 0.7, 0.9, 0.15], dtype=np.float32)
 
-__all__ = ["B200Backend", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
+__all__ = ["B200Backend", "Batch", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
            "library", "pad_geometry", "filter_response", "uniform_angles_deg", "odd_detector_count",
            "phantom_params", "GENERATOR3D_TISSUE", "LIB_PATH"]

@@ -10,16 +10,21 @@
 // reconstruction, denormalised with the slice's span and minimum (span folded
 // into the filter output, minimum added in the epilogue).
 //
-// Work decomposition: a CTA owns a 32 x 32 voxel tile of four slices (the
-// float4 lanes of the filtered rows). Per angle, the detector window that the
-// tile can touch (kBpWindow bins) is staged into shared memory by the bulk-copy
-// engine (cp.async.bulk, completion on an mbarrier), 32 angles per chunk,
-// double-buffered. The tile origin's detector coordinate is evaluated in
+// Work decomposition: a work item is a 32 x 32 voxel tile of four slices (the
+// float4 lanes of the filtered rows) of one job. Per angle, the detector window
+// that the tile can touch (kBpWindow bins) is staged into shared memory by the
+// bulk-copy engine (cp.async.bulk, completion on an mbarrier), 32 angles per
+// chunk, double-buffered. The tile origin's detector coordinate is evaluated in
 // double precision once per angle and split into the window start and a
 // fractional offset, so each thread evaluates u in float on small numbers
 // (|u_local| < 48): the interpolation position is ~10x more accurate than the
 // reference's float u of magnitude ~sq. Each thread accumulates 4 voxels x 4
-// slices in registers.
+// slices in registers; voxels outside the circle load nothing.
+//
+// One kernel serves both shapes of work: a single job with one CTA per item,
+// or a batch of jobs (BpBatch) on a persistent grid that takes items from an
+// atomic counter. An item's arithmetic does not depend on the batch, so a
+// job's output is bit-identical alone and in any mix.
 #include <cmath>
 
 #include "ctb_internal.h"
@@ -64,7 +69,7 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
         "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
     return ok != 0;
 }
-// Bounded wait: gives up after `limit` polls (each poll itself suspends for a
+// Bounded wait: gives up after 2^22 polls (each poll itself suspends for a
 // hardware-defined interval) and reports through the device error word.
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
                                                   unsigned* err) {
@@ -83,20 +88,20 @@ struct AngleRec {
     int pad;
 };
 
-__global__ void __launch_bounds__(THREADS) k_backproject(
-    const float4* __restrict__ filt, int nz, int na, int sq, int guard, int pitch, int n,
-    Trig trig, const float4* __restrict__ stats, int denorm, float* __restrict__ out,
-    unsigned* __restrict__ err) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    auto win = reinterpret_cast<float4 (*)[CA][WIN]>(smem_raw);
-    auto rec = reinterpret_cast<AngleRec (*)[CA]>(smem_raw + sizeof(float4) * NBUF * CA * WIN);
-    auto bar = reinterpret_cast<unsigned long long*>(smem_raw + sizeof(float4) * NBUF * CA * WIN +
-                                                     sizeof(AngleRec) * NBUF * CA);
+struct BpSmem {
+    float4 win[NBUF][CA][WIN];
+    AngleRec rec[NBUF][CA];
+    unsigned long long bar[NBUF];
+};
 
-    const int zg = blockIdx.z;
-    const int x0 = blockIdx.x * TILE, y0 = blockIdx.y * TILE;
+// Backproject one tile (x0, y0) of slice group zg of job J. `chunks` counts
+// the chunks this CTA has consumed so far (mbarrier phases continue across
+// items). Returns false when a bounded wait gave up (block-uniform).
+__device__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x0, int y0, unsigned& chunks,
+                        unsigned* err) {
     const int t = threadIdx.x;
     const int lx = t & 7, ly = t >> 3;
+    const int n = J.n, nz = J.nz, na = J.na, sq = J.sq;
     const int rad = n / 2;
     const float radf = static_cast<float>(rad);
 
@@ -104,7 +109,7 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int z = 4 * zg + j;
-        add[j] = (stats && denorm != CTB_DENORM_NONE && z < nz) ? stats[z].x : 0.0f;
+        add[j] = (J.stats && J.denorm != CTB_DENORM_NONE && z < nz) ? J.stats[z].x : 0.0f;
     }
 
     // Tiles entirely outside the reconstruction circle hold only the offset.
@@ -121,23 +126,17 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int z = 4 * zg + j;
-                    if (z < nz) out[(static_cast<long long>(z) * n + y) * n + x] = add[j];
+                    if (z < nz) J.out[(static_cast<long long>(z) * n + y) * n + x] = add[j];
                 }
             }
-            return;
+            return true;
         }
     }
-
-    if (t == 0) {
-        for (int b = 0; b < NBUF; ++b) mbar_init(&bar[b], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
 
     const double dcd = static_cast<double>(sq / 2);
     const float dcf = static_cast<float>(sq / 2);
     const double ox = static_cast<double>(x0 - rad), oy = static_cast<double>(y0 - rad);
-    const float4* plane = filt + static_cast<long long>(zg) * na * pitch;
+    const float4* plane = J.filt + static_cast<long long>(zg) * na * J.pitch;
     const int nch = (na + CA - 1) / CA;
 
     auto issue = [&](int c, int b) {
@@ -145,8 +144,8 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
         const int cnt = min(CA, na - a0);
         if (t < cnt) {
             const int a = a0 + t;
-            const double2 tc = trig.cs[a];
-            const float2 tf = trig.csf[a];
+            const double2 tc = J.trig.cs[a];
+            const float2 tf = J.trig.csf[a];
             const double uo = ox * tc.x - oy * tc.y + dcd;
             const double umin = uo + fmin(0.0, (TILE - 1) * tc.x) + fmin(0.0, -(TILE - 1) * tc.y);
             const double umax = uo + fmax(0.0, (TILE - 1) * tc.x) + fmax(0.0, -(TILE - 1) * tc.y);
@@ -161,11 +160,11 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
             // taps near bin 0 or bin sq-1: the reference's float u decides them
             r.edge = (umin < 2.0 || umax > sq - 3.0) ? 1 : 0;
             r.pad = 0;
-            rec[b][t] = r;
-            bulk_load(&win[b][t][0], plane + static_cast<long long>(a) * pitch + guard + ws,
-                      WIN * sizeof(float4), &bar[b]);
+            S.rec[b][t] = r;
+            bulk_load(&S.win[b][t][0], plane + static_cast<long long>(a) * J.pitch + J.guard + ws,
+                      WIN * sizeof(float4), &S.bar[b]);
         }
-        if (t == 0) mbar_expect_tx(&bar[b], static_cast<unsigned>(cnt * WIN * sizeof(float4)));
+        if (t == 0) mbar_expect_tx(&S.bar[b], static_cast<unsigned>(cnt * WIN * sizeof(float4)));
     };
 
     float4 acc[4];
@@ -184,19 +183,20 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
         }
     }
 
-    issue(0, 0);
+    // all buffers are idle between items: chunk g of this CTA uses buffer g & 1
+    issue(0, chunks & 1);
     __syncthreads();
-    bool ok_all = true;
     for (int c = 0; c < nch; ++c) {
-        const int b = c & 1;
-        if (c + 1 < nch) issue(c + 1, (c + 1) & 1);
+        const unsigned g = chunks + c;
+        const int b = g & 1;
+        if (c + 1 < nch) issue(c + 1, (g + 1) & 1);
         // A failed wait leaves stale window data; the block then stops as a
         // whole at the barrier below (the decision is block-uniform).
-        const bool landed = mbar_wait_bounded(&bar[b], (c >> 1) & 1, err);
+        const bool landed = mbar_wait_bounded(&S.bar[b], (g >> 1) & 1, err);
         const int cnt = min(CA, na - c * CA);
         for (int j = 0; j < cnt; ++j) {
-            const AngleRec r = rec[b][j];
-            const float4* w = win[b][j];
+            const AngleRec r = S.rec[b][j];
+            const float4* w = S.win[b][j];
             const float ub = fmaf(fx, r.c, fmaf(-fy, r.s, r.f0));
             const float c8 = 8.0f * r.c;
             if (!r.edge) {
@@ -245,25 +245,66 @@ __global__ void __launch_bounds__(THREADS) k_backproject(
                 }
             }
         }
-        if (!__syncthreads_and(landed)) { ok_all = false; break; }
+        if (!__syncthreads_and(landed)) return false;
     }
-    if (!ok_all) return;
+    chunks += nch;
 
     const int y = y0 + ly;
-    const float yy = static_cast<float>(y) - radf;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int x = x0 + lx + 8 * k;
         if (x >= n || y >= n) continue;
-        const float xx = static_cast<float>(x) - radf;
-        const bool inside = !(xx * xx + yy * yy > radf * radf);
+        const bool inside = inside_mask & (1u << k);
         const float v[4] = {acc[k].x, acc[k].y, acc[k].z, acc[k].w};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int z = 4 * zg + j;
-            if (z < nz) out[(static_cast<long long>(z) * n + y) * n + x] = (inside ? v[j] : 0.0f) + add[j];
+            if (z < nz) J.out[(static_cast<long long>(z) * n + y) * n + x] = (inside ? v[j] : 0.0f) + add[j];
         }
     }
+    return true;
+}
+
+// counter == null: one CTA per item (item = blockIdx.x). Otherwise a
+// persistent grid; thread 0 draws items from *counter.
+__global__ void __launch_bounds__(THREADS, 4) k_backproject(const __grid_constant__ BpBatch batch,
+                                                         unsigned long long* __restrict__ counter,
+                                                         unsigned* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    BpSmem& S = *reinterpret_cast<BpSmem*>(smem_raw);
+    __shared__ long long s_item;
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < NBUF; ++b) mbar_init(&S.bar[b], 1);
+        mbar_fence_init();
+    }
+    unsigned chunks = 0;
+    long long item = blockIdx.x;
+    for (;;) {
+        if (counter) {
+            if (threadIdx.x == 0) s_item = static_cast<long long>(atomicAdd(counter, 1ull));
+            __syncthreads();
+            item = s_item;
+        } else {
+            __syncthreads();
+        }
+        if (item >= batch.total) break;
+        int j = 0;
+        while (j + 1 < batch.njobs && batch.job[j + 1].first <= item) ++j;
+        const BpJob& J = batch.job[j];
+        const long long local = item - J.first;
+        const int zg = static_cast<int>(local / J.tiles);
+        const int tl = static_cast<int>(local % J.tiles);
+        if (!bp_tile(S, J, zg, (tl % J.tiles_x) * TILE, (tl / J.tiles_x) * TILE, chunks, err)) break;
+        if (!counter) break;
+        __syncthreads();  // shared state of this item is dead before the next item's staging
+    }
+}
+
+size_t bp_smem() { return sizeof(BpSmem); }
+
+cudaError_t set_bp_smem() {
+    return cudaFuncSetAttribute(k_backproject, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(bp_smem()));
 }
 
 }  // namespace
@@ -287,17 +328,52 @@ FiltLayout filt_layout(int sq, int n_out) {
     return fl;
 }
 
+BpJob make_bp_job(const float4* d_filt, int nz, int na, const FiltLayout& fl, int n_out, Trig trig,
+                  const float4* d_stats, int denorm, float* d_out) {
+    BpJob J;
+    J.filt = d_filt;
+    J.out = d_out;
+    J.stats = d_stats;
+    J.trig = trig;
+    J.nz = nz;
+    J.na = na;
+    J.sq = fl.sq;
+    J.guard = fl.guard;
+    J.pitch = fl.pitch;
+    J.n = n_out;
+    J.denorm = denorm;
+    J.tiles_x = (n_out + TILE - 1) / TILE;
+    J.tiles = J.tiles_x * J.tiles_x;
+    J.first = 0;
+    return J;
+}
+
+cudaError_t launch_backproject_batch(const BpBatch& b, unsigned long long* d_counter,
+                                     unsigned* d_err, cudaStream_t st) {
+    cudaError_t e = set_bp_smem();
+    if (e != cudaSuccess || b.total == 0) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backproject, THREADS, bp_smem());
+    const long long grid = std::min<long long>(b.total, static_cast<long long>(sms) * (per_sm > 0 ? per_sm : 1));
+    e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    k_backproject<<<static_cast<unsigned>(grid), THREADS, bp_smem(), st>>>(b, d_counter, d_err);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltLayout& fl,
                                int n_out, Trig trig, const float4* d_stats, int denorm,
                                float* d_out, unsigned* d_err, cudaStream_t st) {
-    const dim3 grid((n_out + TILE - 1) / TILE, (n_out + TILE - 1) / TILE, (nz + 3) / 4);
-    const size_t smem = sizeof(float4) * NBUF * CA * WIN + sizeof(AngleRec) * NBUF * CA +
-                        sizeof(unsigned long long) * NBUF;
-    const cudaError_t e = cudaFuncSetAttribute(
-        k_backproject, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t e = set_bp_smem();
     if (e != cudaSuccess) return e;
-    k_backproject<<<grid, THREADS, smem, st>>>(d_filt, nz, na, fl.sq, fl.guard, fl.pitch, n_out, trig,
-                                               d_stats, denorm, d_out, d_err);
+    BpBatch b;
+    b.njobs = 1;
+    b.job[0] = make_bp_job(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out);
+    b.total = static_cast<long long>(b.job[0].tiles) * ((nz + 3) / 4);
+    if (b.total > 0x7fffffffLL) return cudaErrorInvalidValue;
+    k_backproject<<<static_cast<unsigned>(b.total), THREADS, bp_smem(), st>>>(b, nullptr, d_err);
     return cudaGetLastError();
 }
 

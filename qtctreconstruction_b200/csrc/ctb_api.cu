@@ -9,7 +9,7 @@
 #include <cstring>
 #include <vector>
 
-#include "ctb_internal.h"
+#include "api_util.h"
 
 namespace ctb {
 cudaError_t launch_phantom_sum_boxes(const float* d_params, const int* d_boxes, int k, int nx,
@@ -44,62 +44,7 @@ void* workspace(ctb_ctx* ctx, const std::string& name, size_t bytes) {
 
 using namespace ctb;
 
-namespace {
-
-constexpr int kMaxAngles = 1 << 16;
-constexpr int kMaxFft = 8192;
-
-ctb_status fail(ctb_ctx* ctx, ctb_status s, const char* fmt, ...) {
-    if (ctx) {
-        char buf[512];
-        va_list ap;
-        va_start(ap, fmt);
-        vsnprintf(buf, sizeof buf, fmt, ap);
-        va_end(ap);
-        ctx->last_error = buf;
-    }
-    return s;
-}
-
-#define CTB_CUDA(ctx, call)                                                                    \
-    do {                                                                                       \
-        const cudaError_t e_ = (call);                                                         \
-        if (e_ != cudaSuccess)                                                                 \
-            return fail((ctx), e_ == cudaErrorMemoryAllocation ? CTB_ERR_OOM : CTB_ERR_CUDA,   \
-                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
-    } while (0)
-
-#define CTB_LAUNCH(ctx, call)       \
-    do {                            \
-        CTB_CUDA(ctx, (call));      \
-        ++(ctx)->launches;          \
-    } while (0)
-
-#define CTB_TRY(expr)                 \
-    do {                              \
-        const ctb_status s_ = (expr); \
-        if (s_ != CTB_OK) return s_;  \
-    } while (0)
-
-template <typename T>
-T* ws(ctb_ctx* ctx, const char* name, size_t count) {
-    return static_cast<T*>(workspace(ctx, name, count * sizeof(T)));
-}
-
-#define CTB_WS(ctx, var, T, name, count)                                                  \
-    T* var = ws<T>((ctx), (name), (count));                                               \
-    if (!var) return fail((ctx), CTB_ERR_OOM, "device workspace '%s' (%zu bytes) failed", \
-                          (name), static_cast<size_t>(count) * sizeof(T))
-
-bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
-
-// Float degrees 180/na * a (SerialBackend.cpp:126-130).
-std::vector<float> uniform_angles(int na) {
-    std::vector<float> a(na);
-    const float step = 180.0f / static_cast<float>(na);
-    for (int i = 0; i < na; ++i) a[i] = step * static_cast<float>(i);
-    return a;
-}
+namespace ctb {
 
 // Fill a device angle table: na double2 (device sincospi) followed by na
 // float2 holding the reference's float cos/sin of degToRad(deg)
@@ -191,12 +136,6 @@ ctb_status filter_tables(ctb_ctx* ctx, const PadGeom& g, int type, const float2*
     return CTB_OK;
 }
 
-struct Guard {
-    ctb_ctx* ctx;
-    std::lock_guard<std::recursive_mutex> lock;
-    explicit Guard(ctb_ctx* c) : ctx(c), lock(c->mu) { cudaSetDevice(c->device); }
-};
-
 ctb_status check_error_word(ctb_ctx* ctx) {
     unsigned h = 0;
     CTB_CUDA(ctx, cudaMemcpyAsync(&h, ctx->d_err, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
@@ -207,6 +146,10 @@ ctb_status check_error_word(ctb_ctx* ctx) {
     }
     return CTB_OK;
 }
+
+}  // namespace ctb
+
+namespace {
 
 // ------------------------------------------------------------ stages
 // Record profiling event `k` of the current set (no-op when `ev` is null).

@@ -98,6 +98,57 @@ cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
                           const FiltLayout& fl, const float2* d_Hc, const float2* d_tw,
                           const float4* d_stats, int denorm, float scale, float4* d_filt,
                           cudaStream_t st);
+
+// ---------------------------------------------------------- batched work
+// A batch is a table of jobs passed by value as a kernel parameter; a
+// persistent grid takes work items from an atomic counter. Each output value
+// is produced by exactly one item with a fixed order of operations, so a job's
+// result does not depend on what else shares the batch.
+constexpr int kMaxJobs = 64;
+
+// Backprojection job: items are (slice group, tile) pairs, slice-group major.
+struct BpJob {
+    const float4* filt;   // [nzg][na][pitch] float4
+    float* out;           // [nz][n][n]
+    const float4* stats;  // per-slice {min, max, ...} or null
+    Trig trig;
+    int nz, na, sq, guard, pitch, n, denorm;
+    int tiles_x, tiles;   // tiles per row / per slice group
+    long long first;      // index of the job's first item in the batch
+};
+struct BpBatch {
+    int njobs = 0;
+    long long total = 0;
+    BpJob job[kMaxJobs];
+};
+// Filtering job: items are (slice pair, angle), slice-pair major. All jobs of a
+// batch share the convolution length Lc (and so the twiddle table).
+struct FiltJob {
+    const float* sino;    // [nz][na][bins]
+    float4* filt;         // [nzg][na][pitch]
+    const float4* stats;
+    const float2* Hc;     // convolution spectrum / Lc
+    int nz, na, bins, sq, pad, guard, pitch, denorm;
+    float scale;
+    long long first;
+};
+struct FiltBatch {
+    int njobs = 0;
+    int Lc = 0;
+    long long total = 0;
+    const float2* tw = nullptr;  // exp(-2 pi i k / Lc)
+    FiltJob job[kMaxJobs];
+};
+BpJob make_bp_job(const float4* d_filt, int nz, int na, const FiltLayout& fl, int n_out, Trig trig,
+                  const float4* d_stats, int denorm, float* d_out);
+FiltJob make_filt_job(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
+                      const float2* d_Hc, const float4* d_stats, int denorm, float scale,
+                      float4* d_filt);
+// Backprojection of a batch on a persistent grid: d_counter (8 bytes, zeroed
+// here on the stream) hands out the items. Filtering takes one CTA per item.
+cudaError_t launch_backproject_batch(const BpBatch& b, unsigned long long* d_counter,
+                                     unsigned* d_err, cudaStream_t st);
+cudaError_t launch_filter_batch(const FiltBatch& b, cudaStream_t st);
 cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltLayout& fl,
                                int n_out, Trig trig, const float4* d_stats, int denorm,
                                float* d_out, unsigned* d_err, cudaStream_t st);

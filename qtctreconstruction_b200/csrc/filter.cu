@@ -13,9 +13,11 @@
 // come back as the real and imaginary parts of IFFT(Hc * FFT(row0 + i row1)).
 // The transform length is the convolution length Lc = nextPow2(sq + nd - 1)
 // (about L/2) with the restricted-lag response Hc (conv_response): the same
-// linear operator as the reference's length-L filtering. A block filters the four
-// slices of a slice group at one angle (two complex FFTs of length L in shared
-// memory, L/16 threads each). The FFT is a radix-16 Stockham transform (one
+// linear operator as the reference's length-L filtering. A block filters two
+// slices at one angle (one complex FFT of length Lc in shared memory, Lc/16
+// threads, Lc/32 past 4096). Blocks read their job from a job table, so one
+// launch filters any number of sinogram stacks that share Lc. The FFT is a
+// radix-16 Stockham transform (one
 // radix-2/4/8 pass when log2 L is not a multiple of 4) with twiddles read
 // from a double-precision-accurate table. Output rows are written as float4
 // (one value per slice), the layout the backprojector stages, scaled by
@@ -293,27 +295,31 @@ __device__ __forceinline__ float slice_scale(const float4* stats, int z, int nz,
     return span > 0.0f ? scale * span : 0.0f;  // OpenMP: span <= 0 -> min everywhere
 }
 
-// grid (na, ceil(nz/2)); block T = L/(16 K) threads filtering slices 2y and
-// 2y+1 at angle x; dynamic smem (L + L/16) float2.
+// One CTA per item (slice pair zp, angle a) of a job of the batch; block
+// T = Lc/(16 K) threads filter slices 2 zp and 2 zp + 1 at angle a; dynamic smem
+// (Lc + Lc/16) float2. An item's arithmetic depends only on its own job.
 template <int K>
-__global__ void __launch_bounds__(256) k_filter(const float* __restrict__ sino, int nz, int na, int nd,
-                                                int sq, int pad, int L, int logL, int guard, int pitch,
-                                                const float2* __restrict__ Hc,
-                                                const float2* __restrict__ tw,
-                                                const float4* __restrict__ stats, int denorm,
-                                                float scale, float4* __restrict__ filt) {
+__global__ void __launch_bounds__(256) k_filter(const __grid_constant__ FiltBatch batch, int logL) {
     extern __shared__ float2 smem[];
-    const int a = blockIdx.x;
-    const int z0 = 2 * blockIdx.y, z1 = z0 + 1;
+    const long long item = blockIdx.x + static_cast<long long>(blockIdx.y) * gridDim.x;
+    if (item >= batch.total) return;
+    int jb = 0;
+    while (jb + 1 < batch.njobs && batch.job[jb + 1].first <= item) ++jb;
+    const FiltJob& J = batch.job[jb];
+    const long long local = item - J.first;
+    const int na = J.na, nz = J.nz, nd = J.bins;
+    const int a = static_cast<int>(local % na);
+    const int z0 = 2 * static_cast<int>(local / na), z1 = z0 + 1;
     const int T = blockDim.x;
     const int tid = threadIdx.x;
-    const float* r0 = sino + (static_cast<long long>(z0) * na + a) * nd;
-    const float* r1 = z1 < nz ? sino + (static_cast<long long>(z1) * na + a) * nd : nullptr;
-    filter_rows<K>(smem, L, logL, tid, T, r0, r1, pad, nd, tw, Hc);
-    const float s0 = slice_scale(stats, z0, nz, denorm, scale);
-    const float s1 = slice_scale(stats, z1, nz, denorm, scale);
+    const float* r0 = J.sino + (static_cast<long long>(z0) * na + a) * nd;
+    const float* r1 = z1 < nz ? J.sino + (static_cast<long long>(z1) * na + a) * nd : nullptr;
+    filter_rows<K>(smem, batch.Lc, logL, tid, T, r0, r1, J.pad, nd, batch.tw, J.Hc);
+    const float s0 = slice_scale(J.stats, z0, nz, J.denorm, J.scale);
+    const float s1 = slice_scale(J.stats, z1, nz, J.denorm, J.scale);
     // rows z0, z1 are lanes (z0 % 4, z0 % 4 + 1) of the float4 layout
-    float2* dst = reinterpret_cast<float2*>(filt + (static_cast<long long>(z0 / 4) * na + a) * pitch) +
+    const int pitch = J.pitch, guard = J.guard, sq = J.sq;
+    float2* dst = reinterpret_cast<float2*>(J.filt + (static_cast<long long>(z0 / 4) * na + a) * pitch) +
                   ((z0 & 3) >> 1);
     for (int i = tid; i < pitch; i += T) {
         const int j = i - guard;
@@ -328,11 +334,30 @@ __global__ void __launch_bounds__(256) k_filter(const float* __restrict__ sino, 
 
 }  // namespace
 
-cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
-                          const FiltLayout& fl, const float2* d_Hc, const float2* d_tw,
-                          const float4* d_stats, int denorm, float scale, float4* d_filt,
-                          cudaStream_t st) {
-    const int L = g.Lc;
+FiltJob make_filt_job(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
+                      const float2* d_Hc, const float4* d_stats, int denorm, float scale,
+                      float4* d_filt) {
+    FiltJob J;
+    J.sino = d_sino;
+    J.filt = d_filt;
+    J.stats = d_stats;
+    J.Hc = d_Hc;
+    J.nz = nz;
+    J.na = na;
+    J.bins = g.bins;
+    J.sq = g.sq;
+    J.pad = g.pad;
+    J.guard = fl.guard;
+    J.pitch = fl.pitch;
+    J.denorm = denorm;
+    J.scale = scale;
+    J.first = 0;
+    return J;
+}
+
+cudaError_t launch_filter_batch(const FiltBatch& b, cudaStream_t st) {
+    const int L = b.Lc;
+    if (b.total == 0) return cudaSuccess;
     int logL = 0;
     while ((1 << logL) < L) ++logL;
     const int K = L > 4096 ? 2 : 1;
@@ -342,10 +367,25 @@ cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    const dim3 grid(na, (nz + 1) / 2);
-    kern<<<grid, threads, smem, st>>>(d_sino, nz, na, g.bins, g.sq, g.pad, L, logL, fl.guard,
-                                      fl.pitch, d_Hc, d_tw, d_stats, denorm, scale, d_filt);
+    // items on a 2-D grid (x up to 65535 wide rows) so totals past 2^31 stay addressable
+    const long long gx = b.total < 65535 ? b.total : 65535;
+    const long long gy = (b.total + gx - 1) / gx;
+    if (gy > 65535) return cudaErrorInvalidValue;
+    kern<<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(gy)), threads, smem, st>>>(b, logL);
     return cudaGetLastError();
+}
+
+cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
+                          const FiltLayout& fl, const float2* d_Hc, const float2* d_tw,
+                          const float4* d_stats, int denorm, float scale, float4* d_filt,
+                          cudaStream_t st) {
+    FiltBatch b;
+    b.njobs = 1;
+    b.Lc = g.Lc;
+    b.tw = d_tw;
+    b.job[0] = make_filt_job(d_sino, nz, na, g, fl, d_Hc, d_stats, denorm, scale, d_filt);
+    b.total = static_cast<long long>(na) * ((nz + 1) / 2);
+    return launch_filter_batch(b, st);
 }
 
 }  // namespace ctb

@@ -1,0 +1,128 @@
+"""Batches of uneven FBP jobs (ctb_batch_* / ctb_fbp_batch_d) on the GPU.
+
+A job's result must not depend on the batch: it is compared bit for bit with
+ctb_fbp_d on the same job alone, with the job alone in a batch, in a mixed
+batch, in the per-job launch mode and replayed from a CUDA graph. One job per
+batch is also checked against the oracle (SerialBackend's float path) within
+the parity tolerance rel-L2 <= 1e-5, max-abs <= 1e-4 * max|f|.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import qtctreconstruction_b200 as ctb
+from qtctreconstruction_b200 import FilterType
+
+pytestmark = pytest.mark.gpu
+
+REL_L2 = 1e-5
+MAX_ABS = 1e-4
+
+# (n_out, depth, num_angles, filter, explicit angles)
+SHAPES = [(64, 16, 101, FilterType.Ramp, False),
+          (96, 5, 151, FilterType.SheppLogan, False),
+          (128, 9, 201, FilterType.Hann, True),
+          (33, 3, 52, FilterType.Ramp, False),
+          (160, 4, 251, FilterType.Hamming, False),
+          (64, 1, 17, FilterType.Bartlett, True),
+          (200, 6, 314, FilterType.Cosine, False)]
+
+
+def _make_jobs(torch, shapes, seed):
+    rng = np.random.default_rng(seed)
+    jobs, host = [], []
+    for n, depth, na, kind, explicit in shapes:
+        nd = ctb.odd_detector_count(n)
+        sino = rng.standard_normal((depth, na, nd)).astype(np.float32)
+        ang = np.sort(rng.uniform(0, 180, na)).astype(np.float32) if explicit else None
+        d_sino = torch.from_numpy(sino).cuda()
+        d_out = torch.full((depth, n, n), float("nan"), dtype=torch.float32, device="cuda")
+        host.append(dict(sino=sino, angles=ang, n=n, kind=kind, d_sino=d_sino, d_out=d_out))
+        jobs.append(dict(sino=d_sino.data_ptr(), depth=depth, num_angles=na, bins=nd, output_size=n,
+                         filter=int(kind), out=d_out.data_ptr(), angles_deg=ang))
+    return jobs, host
+
+
+def _alone(backend, torch, h):
+    depth, na, nd = h["sino"].shape
+    out = torch.zeros((depth, h["n"], h["n"]), dtype=torch.float32, device="cuda")
+    backend.fbp_d(h["d_sino"].data_ptr(), depth, na, nd, h["n"], int(h["kind"]), out.data_ptr(),
+                  angles_deg=h["angles"])
+    backend.synchronize()
+    return out.cpu().numpy()
+
+
+def test_batch_bit_identical_to_single_calls(backend):
+    import torch
+    jobs, host = _make_jobs(torch, SHAPES, 11)
+    backend.fbp_batch_d(jobs)
+    for h in host:
+        got = h["d_out"].cpu().numpy()
+        assert np.all(np.isfinite(got))
+        np.testing.assert_array_equal(got, _alone(backend, torch, h))
+
+
+def test_batch_job_matches_oracle(backend):
+    import torch
+    jobs, host = _make_jobs(torch, SHAPES[1:3], 12)
+    backend.fbp_batch_d(jobs)
+    for h in host:
+        depth, na, nd = h["sino"].shape
+        ang = h["angles"] if h["angles"] is not None else O.uniform_angles_deg(na)
+        got = h["d_out"].cpu().numpy()
+        for z in range(depth):
+            ref = O.reconstruct_slice_f32(h["sino"][z], ang, h["n"], int(h["kind"]))
+            assert O.rel_l2(got[z], ref) <= REL_L2
+            assert O.max_abs_rel(got[z], ref) <= MAX_ABS
+
+
+def test_alone_vs_mixed_and_modes(backend):
+    import torch
+    jobs, host = _make_jobs(torch, SHAPES, 13)
+    target = 2
+    with backend.batch([jobs[target]]) as b:
+        b.run()
+        backend.synchronize()
+    alone = host[target]["d_out"].cpu().numpy().copy()
+    results = {}
+    for flags in (0, ctb.BATCH_GRAPH, ctb.BATCH_PER_JOB, ctb.BATCH_GRAPH | ctb.BATCH_PER_JOB):
+        for h in host:
+            h["d_out"].fill_(float("nan"))
+        with backend.batch(jobs, flags) as b:
+            launches, updates, nbytes = b.info()
+            assert updates == sum(j["output_size"] ** 2 * j["depth"] * j["num_angles"] for j in jobs)
+            if flags & ctb.BATCH_PER_JOB:
+                assert launches == 2 * len(jobs)
+            else:
+                # one filter launch per convolution-length class + one backprojection launch
+                assert 2 <= launches <= len(jobs)
+            for _ in range(2):  # a replay must give the same result
+                b.run()
+            backend.synchronize()
+        results[flags] = [h["d_out"].cpu().numpy().copy() for h in host]
+    np.testing.assert_array_equal(results[0][target], alone)
+    for flags, outs in results.items():
+        for k in range(len(host)):
+            np.testing.assert_array_equal(outs[k], results[0][k])
+
+
+def test_batch_more_jobs_than_one_launch_holds(backend):
+    import torch
+    shapes = [(32 + 8 * (k % 5), 1 + k % 3, 40 + k, FilterType.Ramp, False) for k in range(70)]
+    jobs, host = _make_jobs(torch, shapes, 14)
+    backend.fbp_batch_d(jobs)
+    for h in host[::7]:
+        np.testing.assert_array_equal(h["d_out"].cpu().numpy(), _alone(backend, torch, h))
+
+
+def test_batch_rejects_bad_jobs(backend):
+    import torch
+    jobs, _ = _make_jobs(torch, SHAPES[:2], 15)
+    bad = dict(jobs[1], depth=0)
+    with pytest.raises(ctb.CtbError) as e:
+        backend.fbp_batch_d([jobs[0], bad])
+    assert e.value.status == 1
+    big = dict(jobs[0], bins=4001)  # convolution length 16384
+    with pytest.raises(ctb.CtbError) as e:
+        backend.fbp_batch_d([big])
+    assert e.value.status == 4
