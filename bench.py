@@ -11,7 +11,7 @@ data (no dataset involved); the volume (0.54 GB) exceeds the 126 MB L2, so no
 flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config small|large|medium|precision|batch]
+                  [--config small|large|medium|precision|batch|serving]
 
 N > 1 runs under torch.distributed.run, one rank per GPU, each rank
 reconstructing its own volume (weak scaling; no data-path collective).
@@ -45,6 +45,9 @@ CONFIGS = {
     "batch": dict(jobs=64, seed=4,
                   name="64 uneven FBP jobs: N in {64..768}, 16-256 slices, round(pi/2 N) angles, "
                        "Ram-Lak/Shepp-Logan/Hann, sinograms of seeded 10-ellipsoid phantoms"),
+    "serving": dict(requests=48, seed=5, big_fraction=0.1, budget_gb=120, copy_threads=4, rates=[0.5, 1.0, 2.0, 4.0],
+                    name="Poisson stream of FBP requests: 90% the batch mix, 10% 1024^2 x 64 x 1440 angles; "
+                         "host sinograms in, host volumes out; 120 GB device budget"),
 }
 FILTER_NAMES = ["ramlak", "shepp-logan", "hamming", "cosine", "hann", "bartlett"]
 METRIC = "FBP voxel-angle updates/s"
@@ -459,6 +462,147 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
     return 0
 
 
+# ------------------------------------------------------------------ serving
+def serving_shapes(seed: int, count: int, big_fraction: float):
+    """Request mix: (1 - big_fraction) drawn from the batch distribution, the
+    rest 1024^2 x 64 slices with 1440 angles (Nd 1449), filter as the batch's."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    small = batch_shapes(seed + 1, count)
+    out = []
+    for k in range(count):
+        if rng.random() < big_fraction:
+            out.append(dict(n=1024, nz=64, na=1440, nd=odd_nd(1024), filter=int(rng.choice(BATCH_FILTERS))))
+        else:
+            out.append(small[k])
+    return out
+
+
+def run_plain_stream(be, reqs, arrivals):
+    """One request per call (ctb_fbp on host buffers), in arrival order."""
+    lat, t0 = [], time.perf_counter()
+    for r, a in zip(reqs, arrivals):
+        now = time.perf_counter() - t0
+        if now < a:
+            time.sleep(a - now)
+        s = r["shape"]
+        be.fbp_host_ptr(r["sino"].ctypes.data, s["nz"], s["na"], s["nd"], s["n"], s["filter"], r["out"].ctypes.data)
+        lat.append((time.perf_counter() - t0 - a) * 1e3)
+    span = time.perf_counter() - t0 - arrivals[0]
+    return lat, span
+
+
+def run_served_stream(ctb, reqs, arrivals, budget: int, copy_threads: int):
+    """The same requests through ctb_server: a submitter follows the arrival
+    times; latency is measured by the server from submission to completion."""
+    with ctb.Server(0, memory_budget=budget, copy_threads=copy_threads) as srv:
+        t0 = time.perf_counter()
+        ids = []
+        for r, a in zip(reqs, arrivals):
+            now = time.perf_counter() - t0
+            if now < a:
+                time.sleep(a - now)
+            ids.append(srv.submit(r["sino"], r["shape"]["n"], r["shape"]["filter"], out=r["out"]))
+        status = [srv.wait(i) for i in ids]
+        st = srv.stats()
+    assert all(s == 0 for s in status), status
+    return st
+
+
+def percentile(v, p):
+    v = sorted(v)
+    return v[min(len(v) - 1, max(0, math.ceil(p * len(v)) - 1))]
+
+
+def run_serving(args, cfg, rank: int, world: int, local: int):
+    """Config "serving": a Poisson stream of FBP requests (90 % the batch mix,
+    10 % 1024^2 x 64 x 1440) served two ways on the same GPU from the same host
+    buffers: the plain backend (ctb_fbp, one request per call) and ctb_server
+    (continuous batching, memory-budgeted admission, staged copies). First both
+    at saturation (all requests present at t = 0), then at arrival rates given
+    as multiples of the plain backend's saturated rate."""
+    import numpy as np
+    import torch
+
+    import qtctreconstruction_b200 as ctb
+    torch.cuda.set_device(local)
+    be = ctb.B200Backend(local)
+    shapes = serving_shapes(cfg["seed"], cfg["requests"], cfg["big_fraction"])
+    # sinograms of seeded phantoms, forward-projected on the GPU, kept in host memory
+    reqs = []
+    for k, s in enumerate(shapes):
+        n, nz, na, nd = s["n"], s["nz"], s["na"], s["nd"]
+        vol = torch.empty((nz, n, n), dtype=torch.float32, device="cuda")
+        be.phantom_d(ctb.phantom_params(cfg["seed"] * 1000 + k, 10), n, n, nz, vol.data_ptr())
+        sino = torch.empty((nz, na, nd), dtype=torch.float32, device="cuda")
+        stats = torch.empty((nz, 4), dtype=torch.float32, device="cuda")
+        be.forward_d(vol.data_ptr(), n, nz, na, nd, sino.data_ptr(), stats.data_ptr())
+        be.synchronize()
+        # np.full writes every page now: no first-touch page faults inside a timed run
+        reqs.append(dict(shape=s, sino=sino.cpu().numpy(), out=np.full((nz, n, n), 0.0, np.float32)))
+        del vol, sino
+    torch.cuda.empty_cache()
+    count = len(reqs)
+    vol_bytes = sum(4 * s["nz"] * s["n"] ** 2 for s in shapes)
+    sino_bytes = sum(4 * s["nz"] * s["na"] * s["nd"] for s in shapes)
+    updates = sum(s["n"] ** 2 * s["nz"] * s["na"] for s in shapes)
+    budget = cfg["budget_gb"] << 30
+    # warm-up both paths: the plain backend's workspaces grow to the largest
+    # request first (they are reused, never shrunk), then a few requests each
+    big_s = max(range(count), key=lambda k: reqs[k]["sino"].nbytes)
+    big_o = max(range(count), key=lambda k: reqs[k]["out"].nbytes)
+    for r in [reqs[big_s], reqs[big_o]] + reqs[:args.warmup]:
+        s = r["shape"]
+        be.fbp_host_ptr(r["sino"].ctypes.data, s["nz"], s["na"], s["nd"], s["n"], s["filter"], r["out"].ctypes.data)
+    run_served_stream(ctb, reqs[:args.warmup], [0.0] * args.warmup, budget, cfg["copy_threads"])
+
+    sampler = ClockSampler(gpu_id_for(local))
+    zeros = [0.0] * count
+    lat_p, span_p = run_plain_stream(be, reqs, zeros)
+    plain_sat = count / span_p
+    ref_out = [r["out"].copy() for r in reqs[:3]]
+    st = run_served_stream(ctb, reqs, zeros, budget, cfg["copy_threads"])
+    served_sat = st["volumes_per_s"]
+    same = all(np.array_equal(a, r["out"]) for a, r in zip(ref_out, reqs[:3]))
+    sweep = []
+    rng = np.random.default_rng(cfg["seed"] + 7)
+    for mult in cfg["rates"]:
+        rate = mult * plain_sat
+        arrivals = list(np.cumsum(rng.exponential(1.0 / rate, count)) - 0.0)
+        arrivals = [a - arrivals[0] for a in arrivals]
+        lp, sp = run_plain_stream(be, reqs, arrivals)
+        ss = run_served_stream(ctb, reqs, arrivals, budget, cfg["copy_threads"])
+        sweep.append({"rate_per_s": rate, "rate_x_plain": mult,
+                      "plain": {"volumes_per_s": count / sp, "p50_ms": percentile(lp, 0.5),
+                                "p99_ms": percentile(lp, 0.99)},
+                      "served": {"volumes_per_s": ss["volumes_per_s"], "p50_ms": ss["p50_ms"],
+                                 "p99_ms": ss["p99_ms"], "mean_batch": ss["mean_batch"]}})
+    clocks = sampler.stop()
+    line = {
+        "metric": "volumes/s (mixed FBP request stream)", "value": served_sat, "unit": "volumes/s",
+        "n_gpus": 1, "steps": count, "warmup": args.warmup, "ms_per_step": 1e3 / served_sat,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serving", "description": cfg["name"], "requests": count,
+                   "voxels": vol_bytes // 4, "sinogram_bytes": sino_bytes, "budget_bytes": budget,
+                   "copy_threads": cfg["copy_threads"], "l2": "inputs larger than L2, no flush"},
+        "served": {"volumes_per_s": served_sat, "updates_per_s": st["updates_per_s"], "p50_ms": st["p50_ms"],
+                   "p99_ms": st["p99_ms"], "batches": st["batches"], "mean_batch": st["mean_batch"],
+                   "memory_peak": st["memory_peak"]},
+        "plain": {"volumes_per_s": plain_sat, "updates_per_s": updates / span_p,
+                  "p50_ms": percentile(lat_p, 0.5), "p99_ms": percentile(lat_p, 0.99),
+                  "api": "ctb_fbp, one request per call"},
+        "served_vs_plain": served_sat / plain_sat,
+        "outputs_identical": same,
+        "sweep": sweep,
+        "e2e": {"value": served_sat, "unit": "volumes/s", "h2d_bytes_per_step": sino_bytes // count,
+                "d2h_bytes_per_step": vol_bytes // count},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    be.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -475,11 +619,12 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     cfg = CONFIGS[args.config]
-    if args.config == "batch":
+    if args.config in ("batch", "serving"):
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batch entry point"}))
+            print(json.dumps({"impl": "reference", "unavailable": f"the reference has no {args.config} entry point"}))
             return 0
-        return run_batch(args, cfg, rank, world, local) if rank == 0 else 0
+        run = run_batch if args.config == "batch" else run_serving
+        return run(args, cfg, rank, world, local) if rank == 0 else 0
     if args.impl == "reference":
         return run_reference(args, cfg, rank, world)
     return run_ours(args, cfg, rank, world, local)

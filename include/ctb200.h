@@ -236,6 +236,90 @@ void ctb_batch_destroy(ctb_batch* batch);
 /* ctb_batch_create + run + synchronise + destroy. */
 ctb_status ctb_fbp_batch_d(ctb_ctx* ctx, const ctb_fbp_job* jobs, int njobs);
 
+/* Plain one-request-per-call FBP on host buffers: copy sinos[depth][na][bins]
+ * to the device, filter + backproject into output_size^2 slices (normalised
+ * units), copy the result to out[depth][output_size]^2; returns when done.
+ * The reference's reconstructVolumeFromSinograms with an explicit output size
+ * (BackendFactory.cpp:17-60 reconstructs slice by slice). */
+ctb_status ctb_fbp(ctb_ctx* ctx, const float* sinos, int depth, int num_angles, int bins,
+                   const float* angles_deg, int output_size, int filter, float* out);
+
+/* ------------------------------------------------------------ serving */
+
+/* A serving loop on one GPU (no counterpart in the reference). Requests of
+ * different sizes, angle counts and filters are submitted at any time; a
+ * scheduler thread admits them in arrival order while their device footprint
+ * (sinograms, angle table, filtered rows, volume) fits the memory budget, copy
+ * threads stage host data through pinned buffers on their own streams, and
+ * every scheduling iteration packs the requests whose data is on the device
+ * into one batch (ctb_batch semantics: one filter launch per convolution
+ * length, one persistent backprojection launch) while other requests upload
+ * and download. Results are bit-identical to ctb_fbp_d on the same request. */
+typedef struct ctb_server ctb_server;
+
+typedef struct ctb_server_config {
+    int device;
+    size_t memory_budget;  /* device bytes for request state; 0 = min(120 GB, 85% of free) */
+    int max_batch;         /* requests per batch, 1..64; 0 = 64 */
+    int copy_threads;      /* staging threads per direction; 0 = 4 */
+    size_t staging_bytes;  /* pinned staging per copy thread; 0 = 64 MiB */
+    int fault_every;       /* > 0: every fault_every-th request fails its upload with
+                              CTB_ERR_CUDA (host-side fault injection for tests); 0 = off */
+} ctb_server_config;
+
+enum { CTB_REQ_DEVICE = 1 /* sino and out are device pointers: nothing is staged */ };
+
+typedef struct ctb_request {
+    const float* sino;        /* [depth][num_angles][bins], host unless CTB_REQ_DEVICE */
+    int depth;
+    int num_angles;
+    int bins;
+    const float* angles_deg;  /* host, copied at submit; NULL = uniform 180/na * a */
+    int output_size;
+    int filter;
+    float* out;               /* [depth][output_size]^2, host unless CTB_REQ_DEVICE */
+    int flags;
+} ctb_request;
+
+typedef struct ctb_server_stats {
+    uint64_t submitted, completed, failed, cancelled, rejected;
+    uint64_t batches;         /* batch launches */
+    double mean_batch;        /* requests per batch */
+    double p50_ms, p99_ms, max_ms;  /* submit-to-done latency of completed requests */
+    double volumes_per_s;     /* completed / (last completion - first submission) */
+    double updates_per_s;     /* voxel-angle updates of completed requests over the same span */
+    size_t memory_budget, memory_peak;
+} ctb_server_stats;
+
+ctb_status ctb_server_create(const ctb_server_config* config, ctb_server** out);
+/* Queue a request; *id identifies it. A request whose footprint exceeds the
+ * budget is rejected with CTB_ERR_OOM. The host buffers must stay valid until
+ * the request is final. */
+ctb_status ctb_server_submit(ctb_server* s, const ctb_request* req, uint64_t* id);
+/* CTB_OK when done, CTB_ERR_BUSY while queued or running, the request's error
+ * status if it failed or was cancelled, CTB_ERR_NOT_FOUND for unknown ids. */
+ctb_status ctb_server_poll(ctb_server* s, uint64_t id);
+/* As poll, waiting up to timeout_ms (< 0: no limit). */
+ctb_status ctb_server_wait(ctb_server* s, uint64_t id, double timeout_ms);
+/* Cancel a request: a queued one never runs; a running one finishes on the
+ * device but its result is not copied out. Final status CTB_ERR_CANCELLED. */
+ctb_status ctb_server_cancel(ctb_server* s, uint64_t id);
+/* Forget a final request (its id becomes unknown). */
+ctb_status ctb_server_release(ctb_server* s, uint64_t id);
+ctb_status ctb_server_get_stats(ctb_server* s, ctb_server_stats* out);
+/* Waits for running work, cancels queued requests, frees everything. */
+void ctb_server_destroy(ctb_server* s);
+
+/* The server's admission allocator, usable on its own (host bookkeeping only,
+ * no device calls): first fit over [0, capacity) in 256-byte units, adjacent
+ * free ranges merged. */
+typedef struct ctb_arena ctb_arena;
+ctb_status ctb_arena_create(size_t capacity, ctb_arena** out);
+ctb_status ctb_arena_alloc(ctb_arena* a, size_t bytes, size_t* offset);  /* CTB_ERR_OOM if no fit */
+ctb_status ctb_arena_free(ctb_arena* a, size_t offset);                  /* CTB_ERR_NOT_FOUND */
+ctb_status ctb_arena_stats(const ctb_arena* a, size_t* used, size_t* peak, size_t* largest_free);
+void ctb_arena_destroy(ctb_arena* a);
+
 /* ------------------------------------------------------------ phantoms */
 
 /* Summed random-ellipsoid phantom (the benchmark phantom; a new generator mode

@@ -80,6 +80,29 @@ class FbpJob(ctypes.Structure):
                 ("filter", ctypes.c_int), ("out", ctypes.c_void_p)]
 
 
+class ServerConfig(ctypes.Structure):
+    """ctb_server_config."""
+    _fields_ = [("device", ctypes.c_int), ("memory_budget", ctypes.c_size_t), ("max_batch", ctypes.c_int),
+                ("copy_threads", ctypes.c_int), ("staging_bytes", ctypes.c_size_t), ("fault_every", ctypes.c_int)]
+
+
+class Request(ctypes.Structure):
+    """ctb_request."""
+    _fields_ = [("sino", ctypes.c_void_p), ("depth", ctypes.c_int), ("num_angles", ctypes.c_int),
+                ("bins", ctypes.c_int), ("angles_deg", ctypes.c_void_p), ("output_size", ctypes.c_int),
+                ("filter", ctypes.c_int), ("out", ctypes.c_void_p), ("flags", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    """ctb_server_stats."""
+    _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "completed", "failed", "cancelled", "rejected",
+                                                "batches")] + \
+               [(k, ctypes.c_double) for k in ("mean_batch", "p50_ms", "p99_ms", "max_ms", "volumes_per_s",
+                                               "updates_per_s")] + \
+               [("memory_budget", ctypes.c_size_t), ("memory_peak", ctypes.c_size_t)]
+
+
+REQ_DEVICE = 1     # CTB_REQ_DEVICE
 BATCH_GRAPH = 1    # CTB_BATCH_GRAPH
 BATCH_PER_JOB = 2  # CTB_BATCH_PER_JOB
 
@@ -137,6 +160,23 @@ def _declare(L):
     L.ctb_batch_destroy.argtypes = [p]
     L.ctb_batch_destroy.restype = None
     L.ctb_fbp_batch_d.argtypes = [p, P(FbpJob), i]
+    L.ctb_fbp.argtypes = [p, p, i, i, i, p, i, i, p]
+    L.ctb_server_create.argtypes = [P(ServerConfig), P(p)]
+    L.ctb_server_submit.argtypes = [p, P(Request), P(u64)]
+    L.ctb_server_poll.argtypes = [p, u64]
+    L.ctb_server_wait.argtypes = [p, u64, ctypes.c_double]
+    L.ctb_server_cancel.argtypes = [p, u64]
+    L.ctb_server_release.argtypes = [p, u64]
+    L.ctb_server_get_stats.argtypes = [p, P(ServerStats)]
+    L.ctb_server_destroy.argtypes = [p]
+    L.ctb_server_destroy.restype = None
+    sz = ctypes.c_size_t
+    L.ctb_arena_create.argtypes = [sz, P(p)]
+    L.ctb_arena_alloc.argtypes = [p, sz, P(sz)]
+    L.ctb_arena_free.argtypes = [p, sz]
+    L.ctb_arena_stats.argtypes = [p, P(sz), P(sz), P(sz)]
+    L.ctb_arena_destroy.argtypes = [p]
+    L.ctb_arena_destroy.restype = None
 
 
 # ----------------------------------------------------------------- helpers
@@ -411,6 +451,23 @@ class B200Backend:
         arr._keep = keep
         return arr
 
+    def fbp(self, sinos, output_size: int, kind: int, angles_deg=None) -> np.ndarray:
+        """Plain one-request-per-call FBP on host arrays (ctb_fbp): sinos[depth][na][bins] ->
+        [depth][output_size]^2 in normalised units."""
+        s = _f32(sinos)
+        depth, na, bins = s.shape
+        out = np.empty((depth, output_size, output_size), np.float32)
+        ang = None if angles_deg is None else _f32(angles_deg)
+        self._check(self._lib.ctb_fbp(self._h, s.ctypes.data, depth, na, bins, None if ang is None else ang.ctypes.data,
+                                      output_size, int(kind), out.ctypes.data), "fbp")
+        return out
+
+    def fbp_host_ptr(self, host_sino: int, depth: int, na: int, bins: int, output_size: int, kind: int,
+                     host_out: int):
+        """ctb_fbp on raw host pointers (e.g. preallocated buffers)."""
+        self._check(self._lib.ctb_fbp(self._h, ctypes.c_void_p(host_sino), depth, na, bins, None, output_size,
+                                      int(kind), ctypes.c_void_p(host_out)), "fbp")
+
     def fbp_batch_d(self, jobs):
         """Filter + backproject many device jobs in one batch (ctb_fbp_batch_d); synchronous."""
         arr = self._jobs(jobs)
@@ -465,11 +522,141 @@ class Batch:
         self.close()
 
 
+class Server:
+    """The serving loop (ctb_server_*): submit FBP requests at any time, they are
+    admitted against the device memory budget and run in continuous batches.
+
+    Host requests: ``submit(sino[depth][na][bins], output_size, filter)``; the
+    result array is returned by ``result(id)`` once the request is done.
+    Device requests: ``submit_device(d_sino, depth, na, bins, output_size,
+    filter, d_out)`` with device pointers."""
+
+    def __init__(self, device: int = 0, memory_budget: int = 0, max_batch: int = 0, copy_threads: int = 0,
+                 staging_bytes: int = 0, fault_every: int = 0):
+        self._lib = library()
+        cfg = ServerConfig(device, memory_budget, max_batch, copy_threads, staging_bytes, fault_every)
+        h = ctypes.c_void_p()
+        st = self._lib.ctb_server_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st:
+            raise CtbError(st, "ctb_server_create: " + self._lib.ctb_status_string(st).decode())
+        self._h = h
+        self._keep = {}
+
+    def _submit(self, req: Request, keep) -> int:
+        rid = ctypes.c_uint64()
+        st = self._lib.ctb_server_submit(self._h, ctypes.byref(req), ctypes.byref(rid))
+        if st:
+            raise CtbError(st, "ctb_server_submit: " + self._lib.ctb_status_string(st).decode())
+        self._keep[rid.value] = keep
+        return rid.value
+
+    def submit(self, sino, output_size: int, kind: int, angles_deg=None, out=None) -> int:
+        s = _f32(sino)
+        depth, na, bins = s.shape
+        o = np.empty((depth, output_size, output_size), np.float32) if out is None else out
+        ang = None if angles_deg is None else _f32(angles_deg)
+        req = Request(s.ctypes.data, depth, na, bins, None if ang is None else ang.ctypes.data, output_size,
+                      int(kind), o.ctypes.data, 0)
+        return self._submit(req, (s, o, ang))
+
+    def submit_device(self, d_sino: int, depth: int, na: int, bins: int, output_size: int, kind: int,
+                      d_out: int, angles_deg=None) -> int:
+        ang = None if angles_deg is None else _f32(angles_deg)
+        req = Request(d_sino, depth, na, bins, None if ang is None else ang.ctypes.data, output_size, int(kind),
+                      d_out, REQ_DEVICE)
+        return self._submit(req, (None, None, ang))
+
+    def poll(self, rid: int) -> int:
+        return int(self._lib.ctb_server_poll(self._h, rid))
+
+    def wait(self, rid: int, timeout_ms: float = -1.0) -> int:
+        return int(self._lib.ctb_server_wait(self._h, rid, float(timeout_ms)))
+
+    def cancel(self, rid: int) -> int:
+        return int(self._lib.ctb_server_cancel(self._h, rid))
+
+    def result(self, rid: int, timeout_ms: float = -1.0):
+        """Wait for a host request and return its output array (raises on failure)."""
+        st = self.wait(rid, timeout_ms)
+        if st:
+            raise CtbError(st, self._lib.ctb_status_string(st).decode())
+        return self._keep[rid][1]
+
+    def release(self, rid: int) -> int:
+        st = int(self._lib.ctb_server_release(self._h, rid))
+        if st == 0:
+            self._keep.pop(rid, None)
+        return st
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        st = self._lib.ctb_server_get_stats(self._h, ctypes.byref(s))
+        if st:
+            raise CtbError(st, "ctb_server_get_stats")
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ctb_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Arena:
+    """The server's admission allocator (ctb_arena_*): host bookkeeping only."""
+
+    def __init__(self, capacity: int):
+        self._lib = library()
+        h = ctypes.c_void_p()
+        st = self._lib.ctb_arena_create(capacity, ctypes.byref(h))
+        if st:
+            raise CtbError(st, "ctb_arena_create")
+        self._h = h
+
+    def alloc(self, nbytes: int):
+        """Offset of a new block, or None when nothing fits."""
+        off = ctypes.c_size_t()
+        st = self._lib.ctb_arena_alloc(self._h, nbytes, ctypes.byref(off))
+        return None if st else off.value
+
+    def free(self, offset: int) -> bool:
+        return self._lib.ctb_arena_free(self._h, offset) == 0
+
+    def stats(self):
+        """(used, peak, largest free range) in bytes."""
+        u, p, l = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_size_t()
+        self._lib.ctb_arena_stats(self._h, ctypes.byref(u), ctypes.byref(p), ctypes.byref(l))
+        return u.value, p.value, l.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ctb_arena_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # Generator3D::Params defaults (Generator3D.h:16-34): soft tissue, then bone.
 GENERATOR3D_TISSUE = np.array(
     [-20.0, 45.0, 3.0, 10.0, 0.0, 0.0, 0.0, 1.0,
      200.0, 1000.0, 2.0, 8.0, 1.0, 0.7, 0.9, 0.15], dtype=np.float32)
 
-__all__ = ["B200Backend", "Batch", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
+__all__ = ["B200Backend", "Batch", "Server", "Arena", "ServerConfig", "Request", "ServerStats", "REQ_DEVICE", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
            "library", "pad_geometry", "filter_response", "uniform_angles_deg", "odd_detector_count",
            "phantom_params", "GENERATOR3D_TISSUE", "LIB_PATH"]

@@ -97,7 +97,7 @@ struct BpSmem {
 // Backproject one tile (x0, y0) of slice group zg of job J. `chunks` counts
 // the chunks this CTA has consumed so far (mbarrier phases continue across
 // items). Returns false when a bounded wait gave up (block-uniform).
-__device__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x0, int y0, unsigned& chunks,
+__device__ __forceinline__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x0, int y0, unsigned& chunks,
                         unsigned* err) {
     const int t = threadIdx.x;
     const int lx = t & 7, ly = t >> 3;
@@ -265,37 +265,42 @@ __device__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x0, int y0, unsig
     return true;
 }
 
-// counter == null: one CTA per item (item = blockIdx.x). Otherwise a
-// persistent grid; thread 0 draws items from *counter.
+// PERSISTENT = false: one CTA per item (item = blockIdx.x). Otherwise a
+// persistent grid whose thread 0 draws items from *counter.
+template <bool PERSISTENT>
 __global__ void __launch_bounds__(THREADS, 4) k_backproject(const __grid_constant__ BpBatch batch,
-                                                         unsigned long long* __restrict__ counter,
-                                                         unsigned* __restrict__ err) {
+                                                            unsigned* __restrict__ counter,
+                                                            unsigned* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     BpSmem& S = *reinterpret_cast<BpSmem*>(smem_raw);
-    __shared__ long long s_item;
+    __shared__ int s_item;
     if (threadIdx.x == 0) {
         for (int b = 0; b < NBUF; ++b) mbar_init(&S.bar[b], 1);
         mbar_fence_init();
     }
     unsigned chunks = 0;
-    long long item = blockIdx.x;
+    if (!PERSISTENT) {
+        // one item per CTA; job 0 indexed statically keeps its fields
+        // constant-bank operands instead of registers
+        __syncthreads();
+        const BpJob& J = batch.job[0];
+        const int zg = blockIdx.x / J.tiles;
+        const int tl = blockIdx.x - zg * J.tiles;
+        bp_tile(S, J, zg, (tl % J.tiles_x) * TILE, (tl / J.tiles_x) * TILE, chunks, err);
+        return;
+    }
     for (;;) {
-        if (counter) {
-            if (threadIdx.x == 0) s_item = static_cast<long long>(atomicAdd(counter, 1ull));
-            __syncthreads();
-            item = s_item;
-        } else {
-            __syncthreads();
-        }
+        if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));
+        __syncthreads();
+        const int item = s_item;  // totals are below 2^31 (checked at launch)
         if (item >= batch.total) break;
         int j = 0;
         while (j + 1 < batch.njobs && batch.job[j + 1].first <= item) ++j;
         const BpJob& J = batch.job[j];
-        const long long local = item - J.first;
-        const int zg = static_cast<int>(local / J.tiles);
-        const int tl = static_cast<int>(local % J.tiles);
+        const int local = item - static_cast<int>(J.first);
+        const int zg = local / J.tiles;
+        const int tl = local - zg * J.tiles;
         if (!bp_tile(S, J, zg, (tl % J.tiles_x) * TILE, (tl / J.tiles_x) * TILE, chunks, err)) break;
-        if (!counter) break;
         __syncthreads();  // shared state of this item is dead before the next item's staging
     }
 }
@@ -303,7 +308,10 @@ __global__ void __launch_bounds__(THREADS, 4) k_backproject(const __grid_constan
 size_t bp_smem() { return sizeof(BpSmem); }
 
 cudaError_t set_bp_smem() {
-    return cudaFuncSetAttribute(k_backproject, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_backproject<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(bp_smem()));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_backproject<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(bp_smem()));
 }
 
@@ -348,18 +356,19 @@ BpJob make_bp_job(const float4* d_filt, int nz, int na, const FiltLayout& fl, in
     return J;
 }
 
-cudaError_t launch_backproject_batch(const BpBatch& b, unsigned long long* d_counter,
-                                     unsigned* d_err, cudaStream_t st) {
+cudaError_t launch_backproject_batch(const BpBatch& b, unsigned* d_counter, unsigned* d_err,
+                                     cudaStream_t st) {
     cudaError_t e = set_bp_smem();
     if (e != cudaSuccess || b.total == 0) return e;
+    if (b.total > 0x7fffffffLL) return cudaErrorInvalidValue;
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backproject, THREADS, bp_smem());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backproject<true>, THREADS, bp_smem());
     const long long grid = std::min<long long>(b.total, static_cast<long long>(sms) * (per_sm > 0 ? per_sm : 1));
-    e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st);
+    e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
-    k_backproject<<<static_cast<unsigned>(grid), THREADS, bp_smem(), st>>>(b, d_counter, d_err);
+    k_backproject<true><<<static_cast<unsigned>(grid), THREADS, bp_smem(), st>>>(b, d_counter, d_err);
     return cudaGetLastError();
 }
 
@@ -373,7 +382,7 @@ cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltL
     b.job[0] = make_bp_job(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out);
     b.total = static_cast<long long>(b.job[0].tiles) * ((nz + 3) / 4);
     if (b.total > 0x7fffffffLL) return cudaErrorInvalidValue;
-    k_backproject<<<static_cast<unsigned>(b.total), THREADS, bp_smem(), st>>>(b, nullptr, d_err);
+    k_backproject<false><<<static_cast<unsigned>(b.total), THREADS, bp_smem(), st>>>(b, nullptr, d_err);
     return cudaGetLastError();
 }
 

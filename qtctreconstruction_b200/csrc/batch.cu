@@ -28,7 +28,7 @@ struct ctb_batch {
     std::vector<BpBatch> bp;      // one launch each
     void* mem = nullptr;          // angle tables + filtered rows of every job
     size_t bytes = 0;
-    unsigned long long* d_counter = nullptr;
+    unsigned* d_counter = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int kernel_launches = 0;
@@ -105,7 +105,7 @@ ctb_status build(ctb_batch* b) {
     b->bytes = off;
     CTB_CUDA(ctx, cudaMalloc(&b->mem, off));
     char* base = static_cast<char*>(b->mem);
-    b->d_counter = reinterpret_cast<unsigned long long*>(base);
+    b->d_counter = reinterpret_cast<unsigned*>(base);
 
     std::vector<FiltJob> fj(n);
     std::vector<BpJob> bj(n);

@@ -559,6 +559,30 @@ ctb_status ctb_reconstruct_from_sinograms(ctb_ctx* ctx, const float* sinos, int 
     return check_error_word(ctx);
 }
 
+ctb_status ctb_fbp(ctb_ctx* ctx, const float* sinos, int depth, int num_angles, int bins,
+                   const float* angles_deg, int output_size, int filter, float* out) {
+    CTB_TRY(check_common(ctx));
+    if (!sinos || !out || depth <= 0 || num_angles <= 0 || num_angles > kMaxAngles || bins <= 0 ||
+        output_size <= 0 || filter < 0 || filter > CTB_FILTER_BARTLETT)
+        return fail(ctx, CTB_ERR_INVALID, "ctb_fbp: invalid arguments");
+    Guard g(ctx);
+    const size_t ns = static_cast<size_t>(depth) * num_angles * bins;
+    const size_t no = static_cast<size_t>(depth) * output_size * output_size;
+    CTB_WS(ctx, d_sino, float, "h_sino", ns);
+    CTB_WS(ctx, d_out, float, "h_out", no);
+    CTB_CUDA(ctx, cudaMemcpyAsync(d_sino, sinos, ns * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+    CTB_TRY(fbp_stage(ctx, d_sino, depth, num_angles, bins, angles_deg, output_size, filter, nullptr,
+                      CTB_DENORM_NONE, d_out));
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+    CTB_CUDA(ctx, cudaMemcpyAsync(out, d_out, no * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+    ctx->last_recon_ms = ms;
+    return check_error_word(ctx);
+}
+
 // ------------------------------------------------------------------ phantoms
 ctb_status ctb_phantom_params(uint64_t seed, int count, float* params) {
     if (count < 0 || (count > 0 && !params)) return CTB_ERR_INVALID;
