@@ -99,6 +99,17 @@ uint64_t ctb_launch_count(const ctb_ctx* ctx);
 ctb_status ctb_set_profiling(ctb_ctx* ctx, int enable);
 ctb_status ctb_stage_times(ctb_ctx* ctx, int back, double* ms);
 
+/* Filter implementation of the context's filter stages (ctb_reconstruct_*,
+ * ctb_fbp*, the _d variants; batches and the serving loop always use the FFT):
+ *   FFT         the radix-16 shared-memory FFT convolution in FP32 (default);
+ *   TC_BF16X3   the same linear operator as a dense Toeplitz-matrix product on
+ *               the tcgen05 tensor cores, both factors split into two BF16
+ *               terms, three products accumulated in FP32 (the precision
+ *               option; the dropped low x low term is about 2^-16 relative).
+ * The reference filters with its own radix-2 FFT (FFT.cpp:9-158). */
+enum { CTB_FILTER_MODE_FFT = 0, CTB_FILTER_MODE_TC_BF16X3 = 1 };
+ctb_status ctb_set_filter_mode(ctb_ctx* ctx, int mode);
+
 /* Measured shared-memory load bandwidth of this GPU in GB/s: a conflict-free
  * 16-byte-per-lane load loop over all SMs, timed with CUDA events. The
  * backprojector's roofline denominator. */

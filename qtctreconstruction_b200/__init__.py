@@ -103,6 +103,8 @@ class ServerStats(ctypes.Structure):
 
 
 REQ_DEVICE = 1     # CTB_REQ_DEVICE
+FILTER_MODE_FFT = 0         # CTB_FILTER_MODE_FFT
+FILTER_MODE_TC_BF16X3 = 1   # CTB_FILTER_MODE_TC_BF16X3
 BATCH_GRAPH = 1    # CTB_BATCH_GRAPH
 BATCH_PER_JOB = 2  # CTB_BATCH_PER_JOB
 
@@ -152,6 +154,7 @@ def _declare(L):
     L.ctb_generator3d.argtypes = [p, i, i, i, f, i, ctypes.c_uint32, _F32P, p]
     L.ctb_extract_point_cloud.argtypes = [p, p, i, i, i, f, p, ctypes.c_int64, P(ctypes.c_int64)]
     L.ctb_set_profiling.argtypes = [p, i]
+    L.ctb_set_filter_mode.argtypes = [p, i]
     L.ctb_stage_times.argtypes = [p, i, P(ctypes.c_double)]
     L.ctb_probe_smem_bandwidth.argtypes = [p, P(ctypes.c_double)]
     L.ctb_batch_create.argtypes = [p, P(FbpJob), i, i, P(p)]
@@ -416,6 +419,10 @@ class B200Backend:
         self._check(self._lib.ctb_reconstruct_volume(self._h, ctypes.c_void_p(host_vol), n, depth, na, nd,
                                                      int(kind), ctypes.c_void_p(host_out)), "reconstructVolume")
 
+    def set_filter_mode(self, mode: int):
+        """FILTER_MODE_FFT (default) or FILTER_MODE_TC_BF16X3 (tensor-core Toeplitz product)."""
+        self._check(self._lib.ctb_set_filter_mode(self._h, int(mode)), "set_filter_mode")
+
     def set_profiling(self, enable: bool = True):
         self._check(self._lib.ctb_set_profiling(self._h, int(bool(enable))), "set_profiling")
 
@@ -657,6 +664,6 @@ GENERATOR3D_TISSUE = np.array(
     [-20.0, 45.0, 3.0, 10.0, 0.0, 0.0, 0.0, 1.0,
      200.0, 1000.0, 2.0, 8.0, 1.0, 0.7, 0.9, 0.15], dtype=np.float32)
 
-__all__ = ["B200Backend", "Batch", "Server", "Arena", "ServerConfig", "Request", "ServerStats", "REQ_DEVICE", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
+__all__ = ["FILTER_MODE_FFT", "FILTER_MODE_TC_BF16X3", "B200Backend", "Batch", "Server", "Arena", "ServerConfig", "Request", "ServerStats", "REQ_DEVICE", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
            "library", "pad_geometry", "filter_response", "uniform_angles_deg", "odd_detector_count",
            "phantom_params", "GENERATOR3D_TISSUE", "LIB_PATH"]

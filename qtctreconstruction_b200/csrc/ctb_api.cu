@@ -230,8 +230,22 @@ ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins
     CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
     // SerialBackend.cpp:246: pi / (2 na) in float
     const float scale = 3.14159265358979323846f / (2.0f * static_cast<float>(na));
-    CTB_LAUNCH(ctx, launch_filter(d_sino, nz, na, g, fl, d_Hc, d_tw, d_stats, denorm, scale, d_filt,
-                                  ctx->stream));
+    if (ctx->filter_mode == CTB_FILTER_MODE_TC_BF16X3) {
+        const auto key = std::make_pair(bins, filter);
+        auto it = ctx->gemm_tables.find(key);
+        if (it == ctx->gemm_tables.end()) {
+            GemmTable tab;
+            CTB_CUDA(ctx, make_gemm_table(g, filter, &tab));
+            it = ctx->gemm_tables.emplace(key, tab).first;
+        }
+        CTB_WS(ctx, d_split, unsigned char, "gemm_split", filter_gemm_split_bytes(nz, na, bins));
+        CTB_CUDA(ctx, launch_filter_gemm(d_sino, nz, na, g, fl, it->second, d_stats, denorm, scale, d_filt,
+                                         d_split, ctx->d_err, ctx->stream));
+        ctx->launches += 2;
+    } else {
+        CTB_LAUNCH(ctx, launch_filter(d_sino, nz, na, g, fl, d_Hc, d_tw, d_stats, denorm, scale, d_filt,
+                                      ctx->stream));
+    }
     mark(ctx, ev, 3);
     CTB_LAUNCH(ctx, launch_backproject(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out,
                                        ctx->d_err, ctx->stream));
@@ -301,6 +315,7 @@ void ctb_destroy(ctb_ctx* ctx) {
         for (auto& kv : ctx->ws) cudaFree(kv.second.ptr);
         for (auto& kv : ctx->filters) cudaFree(kv.second.ptr);
         for (auto& kv : ctx->twiddles) cudaFree(kv.second.ptr);
+        for (auto& kv : ctx->gemm_tables) cudaFree(kv.second.T.ptr);
         for (auto& kv : ctx->trig_uniform) cudaFree(kv.second.ptr);
         for (auto& kv : ctx->fwd_plans) {
             cudaFree(kv.second.groups.ptr);
@@ -349,6 +364,13 @@ ctb_status ctb_filter_response(int fft_size, int filter, float* H) {
     if (fft_size < 2 || (fft_size & (fft_size - 1)) || !H) return CTB_ERR_INVALID;
     const auto v = filter_response(fft_size, filter);
     for (size_t i = 0; i < v.size(); ++i) H[i] = static_cast<float>(v[i]);
+    return CTB_OK;
+}
+
+ctb_status ctb_set_filter_mode(ctb_ctx* ctx, int mode) {
+    if (!ctx || (mode != CTB_FILTER_MODE_FFT && mode != CTB_FILTER_MODE_TC_BF16X3)) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    ctx->filter_mode = mode;
     return CTB_OK;
 }
 

@@ -30,6 +30,10 @@ PadGeom pad_geometry(int bins);
 // Lc with h restricted to those lags. Returns DFT_Lc of that kernel divided by Lc
 // (re, im interleaved), evaluated in double precision.
 std::vector<double> conv_response(const PadGeom& g, int type);
+// The same kernel in the lag domain: h(d) for d = -(pad + bins - 1) .. sq - 1 - pad
+// (index d + pad + bins - 1), double precision. Filtered bin i of a row x is
+// sum_j h(i - pad - j) x[j].
+std::vector<double> conv_kernel(const PadGeom& g, int type);
 
 // Layout of the filtered rows the backprojector reads: for each group of four
 // slices and each angle, `pitch` bins of float4 (one float per slice), with
@@ -98,6 +102,24 @@ cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
                           const FiltLayout& fl, const float2* d_Hc, const float2* d_tw,
                           const float4* d_stats, int denorm, float scale, float4* d_filt,
                           cudaStream_t st);
+
+// ------------------------------------------------ tensor-core filter option
+// Toeplitz filter matrix T[i][j] = h(i - pad - j) split into two BF16 terms
+// (rows padded to ntiles * bn, columns to kpad), with the TMA tensor maps of
+// both halves (opaque CUtensorMap bytes).
+struct GemmTable {
+    DevBuf T;
+    int bn = 0, ntiles = 0, nrows = 0, kpad = 0;
+    alignas(64) unsigned char map_hi[128];
+    alignas(64) unsigned char map_lo[128];
+};
+cudaError_t make_gemm_table(const PadGeom& g, int type, GemmTable* out);
+int gemm_kpad(int bins);
+// Device bytes of the BF16 row split the tensor-core filter needs.
+size_t filter_gemm_split_bytes(int nz, int na, int bins);
+cudaError_t launch_filter_gemm(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
+                               const GemmTable& tab, const float4* d_stats, int denorm, float scale,
+                               float4* d_filt, void* d_split, unsigned* d_err, cudaStream_t st);
 
 // ---------------------------------------------------------- batched work
 // A batch is a table of jobs passed by value as a kernel parameter; a
@@ -182,6 +204,10 @@ struct ctb_ctx {
     // Cached tables: filter spectra per (L, type), twiddles per L.
     std::map<std::pair<int, int>, ctb::DevBuf> filters;
     std::map<int, ctb::DevBuf> twiddles;
+    // Filter implementation (ctb_set_filter_mode) and the tensor-core path's
+    // Toeplitz tables per (bins, filter).
+    int filter_mode = 0;
+    std::map<std::pair<int, int>, ctb::GemmTable> gemm_tables;
     // Angle tables: uniform angle sets per count; the last explicit list.
     std::map<int, ctb::DevBuf> trig_uniform;
     std::vector<float> user_angles;

@@ -54,8 +54,8 @@ PadGeom pad_geometry(int bins) {
     return g;
 }
 
-std::vector<double> conv_response(const PadGeom& g, int type) {
-    const int L = g.L, Lc = g.Lc;
+std::vector<double> conv_kernel(const PadGeom& g, int type) {
+    const int L = g.L;
     const std::vector<double> H = filter_response(L, type);
     // h = IDFT_L(H~): H~ is real and even, so h = Re FFT_L(H~) / L (real, even)
     std::vector<std::complex<double>> t(L);
@@ -63,11 +63,20 @@ std::vector<double> conv_response(const PadGeom& g, int type) {
     t[0] = 0.0;
     t[L / 2] = 0.0;
     fft64(t);
-    std::vector<std::complex<double>> hc(Lc, 0.0);
     const int dmin = -(g.pad + g.bins - 1), dmax = g.sq - 1 - g.pad;
-    for (int d = dmin; d <= dmax; ++d) {
-        const double hv = t[((d % L) + L) % L].real() / L;
-        hc[((d % Lc) + Lc) % Lc] = hv;
+    std::vector<double> h(dmax - dmin + 1);
+    for (int d = dmin; d <= dmax; ++d) h[d - dmin] = t[((d % L) + L) % L].real() / L;
+    return h;
+}
+
+std::vector<double> conv_response(const PadGeom& g, int type) {
+    const int Lc = g.Lc;
+    const std::vector<double> h = conv_kernel(g, type);
+    std::vector<std::complex<double>> hc(Lc, 0.0);
+    const int dmin = -(g.pad + g.bins - 1);
+    for (size_t k = 0; k < h.size(); ++k) {
+        const int d = dmin + static_cast<int>(k);
+        hc[((d % Lc) + Lc) % Lc] = h[k];
     }
     fft64(hc);
     std::vector<double> out(2 * static_cast<size_t>(Lc));
