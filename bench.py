@@ -284,6 +284,7 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / args.steps
     stages = np.mean([be.stage_times(back) for back in range(args.steps)], axis=0)
+    filt_kernel_ms = float(np.mean([be.filter_kernel_ms(back) for back in range(args.steps)]))
 
     # ---- end to end through the host-buffer C ABI call (pinned host buffers)
     hin = torch.empty((nz, n, n), dtype=torch.float32, pin_memory=True)
@@ -344,15 +345,17 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
                          "peak_source": "measured shared-memory load bandwidth (probe kernel, same run)",
                          "algorithmic": "8 B (two float taps) per in-circle voxel-angle update"},
             "roofline_filter": {"kernel": "k_filter", "bound": "hbm",
-                                "achieved": filt_bytes / (stages[2] * 1e-3) / 1e9,
+                                "achieved": filt_bytes / (filt_kernel_ms * 1e-3) / 1e9,
                                 "peak": hbm_peak, "unit": "GB/s",
-                                "frac": (filt_bytes / (stages[2] * 1e-3) / 1e9 / hbm_peak) if hbm_peak else None,
+                                "frac": (filt_bytes / (filt_kernel_ms * 1e-3) / 1e9 / hbm_peak) if hbm_peak else None,
                                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_peak else None},
             "e2e": {"value": world * updates / (e2e_ms * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": 4 * n * n * nz, "d2h_bytes_per_step": 4 * n * n * nz,
                     "ms_per_step": e2e_ms, "api": "ctb_reconstruct_volume (pinned host buffers)"},
             "clocks": clocks,
         }
+        if args.filter_modes:
+            line["filter_modes"] = filter_mode_report(args, cfg, be, stream, vol, out, params, peaks)
         if world == 1 and not args.no_cpu_baseline:
             r, threads, kind_b, isa, sample = cpu_reference_rate(cfg, args.ref_slices, params)
             line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": threads, "kind": kind_b,
@@ -363,6 +366,67 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+# ------------------------------------------------------------- filter modes
+def filter_mode_report(args, cfg, be, stream, vol, out, params, peaks):
+    """The two filter implementations on the config's volume: device time of
+    the filter stage and of its main kernel (CUDA events, profiled steps),
+    the tensor-core product's roofline, and the error of each against the
+    FP64 rerun of SerialBackend on two slices (sinograms from the GPU forward
+    projector, reconstructed by each filter mode and by the FP64 oracle)."""
+    import numpy as np
+    import torch
+
+    import oracle as O
+    import qtctreconstruction_b200 as ctb
+    n, nz, na, kind = cfg["n"], cfg["nz"], cfg["na"], cfg["filter"]
+    nd = odd_nd(n)
+    sq = math.ceil(math.sqrt(2.0) * nd)
+    steps = max(3, args.steps // 2)
+    rep = {}
+    for name, mode in (("fft", ctb.FILTER_MODE_FFT), ("tc_bf16x3", ctb.FILTER_MODE_TC_BF16X3)):
+        be.set_filter_mode(mode)
+        for _ in range(2):
+            be.reconstruct_volume_d(vol.data_ptr(), n, nz, na, nd, kind, out.data_ptr())
+        for _ in range(steps):
+            be.reconstruct_volume_d(vol.data_ptr(), n, nz, na, nd, kind, out.data_ptr())
+        torch.cuda.synchronize()
+        st = np.mean([be.stage_times(b) for b in range(steps)], axis=0)
+        km = float(np.mean([be.filter_kernel_ms(b) for b in range(steps)]))
+        rep[name] = {"filter_stage_ms": float(st[2]), "main_kernel_ms": km}
+    be.set_filter_mode(ctb.FILTER_MODE_FFT)
+    flops = 3 * 2.0 * nz * na * nd * sq
+    tc_ms = rep["tc_bf16x3"]["main_kernel_ms"]
+    peak = peaks.get("bf16_tflops_sustained")
+    rep["tc_bf16x3"]["roofline"] = {
+        "kernel": "k_filter_gemm", "bound": "tensor", "achieved": flops / (tc_ms * 1e-3) / 1e12, "peak": peak,
+        "unit": "TFLOP/s", "frac": (flops / (tc_ms * 1e-3) / 1e12 / peak) if peak else None,
+        "algorithmic": "3 x 2 x rows x nd x sq FLOP (three BF16 products of the Toeplitz filter)",
+        "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured; the kernel runs inside a long step)"}
+    # accuracy on two slices against the FP64 rerun
+    z0 = nz // 2
+    slab = torch.from_numpy(O.phantom_sum_slab(params, n, n, nz, z0, 2)).cuda()
+    d_sino = torch.empty((2, na, nd), dtype=torch.float32, device="cuda")
+    d_stats = torch.empty((2, 4), dtype=torch.float32, device="cuda")
+    be.forward_d(slab.data_ptr(), n, 2, na, nd, d_sino.data_ptr(), d_stats.data_ptr())
+    be.synchronize()
+    sino = d_sino.cpu().numpy()
+    ang = O.uniform_angles_deg(na)
+    f64 = [O.reconstruct_slice_f64(sino[z], ang, n, kind) for z in range(2)]
+    d_out = torch.empty((2, n, n), dtype=torch.float32, device="cuda")
+    for name, mode in (("fft", ctb.FILTER_MODE_FFT), ("tc_bf16x3", ctb.FILTER_MODE_TC_BF16X3)):
+        be.set_filter_mode(mode)
+        be.fbp_d(d_sino.data_ptr(), 2, na, nd, n, kind, d_out.data_ptr())
+        be.synchronize()
+        got = d_out.cpu().numpy()
+        rep[name]["rel_l2_vs_fp64"] = max(O.rel_l2(got[z], f64[z]) for z in range(2))
+        rep[name]["max_abs_vs_fp64"] = max(O.max_abs_rel(got[z], f64[z]) for z in range(2))
+    be.set_filter_mode(ctb.FILTER_MODE_FFT)
+    rep["default"] = "fft"
+    rep["rule"] = "the tensor-core product is used only where it beats the FFT path at <= 1e-5 rel-L2 vs FP64"
+    rep["accuracy_sample"] = f"slices {z0}, {z0 + 1}: GPU forward projection, FBP per mode vs FP64 oracle"
+    return rep
 
 
 # ------------------------------------------------------------------ batches
@@ -612,6 +676,8 @@ def main():
     ap.add_argument("--config", choices=sorted(CONFIGS), default="large")
     ap.add_argument("--ref-slices", type=int, default=2, help="slices per CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--filter-modes", action="store_true",
+                    help="also time the tensor-core filter and compare both filters with FP64 (default for precision)")
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
@@ -619,6 +685,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     cfg = CONFIGS[args.config]
+    if args.config == "precision":
+        args.filter_modes = True
     if args.config in ("batch", "serving"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": f"the reference has no {args.config} entry point"}))

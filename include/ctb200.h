@@ -98,6 +98,9 @@ uint64_t ctb_launch_count(const ctb_ctx* ctx);
  * normalisation, forward projection, filtering, backprojection}. */
 ctb_status ctb_set_profiling(ctb_ctx* ctx, int enable);
 ctb_status ctb_stage_times(ctb_ctx* ctx, int back, double* ms);
+/* Device ms of the filter stage's main kernel alone in the same profiled call
+ * (the FFT kernel, or the tensor-core product without its operand split). */
+ctb_status ctb_filter_kernel_ms(ctb_ctx* ctx, int back, double* ms);
 
 /* Filter implementation of the context's filter stages (ctb_reconstruct_*,
  * ctb_fbp*, the _d variants; batches and the serving loop always use the FFT):

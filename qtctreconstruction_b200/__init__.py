@@ -155,6 +155,7 @@ def _declare(L):
     L.ctb_extract_point_cloud.argtypes = [p, p, i, i, i, f, p, ctypes.c_int64, P(ctypes.c_int64)]
     L.ctb_set_profiling.argtypes = [p, i]
     L.ctb_set_filter_mode.argtypes = [p, i]
+    L.ctb_filter_kernel_ms.argtypes = [p, i, P(ctypes.c_double)]
     L.ctb_stage_times.argtypes = [p, i, P(ctypes.c_double)]
     L.ctb_probe_smem_bandwidth.argtypes = [p, P(ctypes.c_double)]
     L.ctb_batch_create.argtypes = [p, P(FbpJob), i, i, P(p)]
@@ -431,6 +432,12 @@ class B200Backend:
         t = (ctypes.c_double * 4)()
         self._check(self._lib.ctb_stage_times(self._h, back, t), "stage_times")
         return list(t)
+
+    def filter_kernel_ms(self, back: int = 0) -> float:
+        """Device ms of the filter's main kernel in a profiled volume call."""
+        t = ctypes.c_double()
+        self._check(self._lib.ctb_filter_kernel_ms(self._h, back, ctypes.byref(t)), "filter_kernel_ms")
+        return t.value
 
     def probe_smem_bandwidth(self) -> float:
         g = ctypes.c_double()

@@ -239,10 +239,12 @@ ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins
             it = ctx->gemm_tables.emplace(key, tab).first;
         }
         CTB_WS(ctx, d_split, unsigned char, "gemm_split", filter_gemm_split_bytes(nz, na, bins));
-        CTB_CUDA(ctx, launch_filter_gemm(d_sino, nz, na, g, fl, it->second, d_stats, denorm, scale, d_filt,
-                                         d_split, ctx->d_err, ctx->stream));
-        ctx->launches += 2;
+        CTB_LAUNCH(ctx, launch_filter_gemm_prep(d_sino, nz, na, g, fl, it->second, d_filt, d_split, ctx->stream));
+        mark(ctx, ev, 5);
+        CTB_LAUNCH(ctx, launch_filter_gemm(d_sino, nz, na, g, fl, it->second, d_stats, denorm, scale, d_filt,
+                                           d_split, ctx->d_err, ctx->stream));
     } else {
+        mark(ctx, ev, 5);
         CTB_LAUNCH(ctx, launch_filter(d_sino, nz, na, g, fl, d_Hc, d_tw, d_stats, denorm, scale, d_filt,
                                       ctx->stream));
     }
@@ -392,12 +394,26 @@ ctb_status ctb_stage_times(ctb_ctx* ctx, int back, double* ms) {
     Guard g(ctx);
     const long long idx = (ctx->prof_calls - 1 - back) % ctb_ctx::kProfRing;
     cudaEvent_t* ev = &ctx->prof_ev[idx * ctb_ctx::kProfEvents];
-    CTB_CUDA(ctx, cudaEventSynchronize(ev[ctb_ctx::kProfEvents - 1]));
-    for (int k = 0; k + 1 < ctb_ctx::kProfEvents; ++k) {
+    CTB_CUDA(ctx, cudaEventSynchronize(ev[4]));
+    for (int k = 0; k < 4; ++k) {
         float t = 0.f;
         CTB_CUDA(ctx, cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
         ms[k] = t;
     }
+    return CTB_OK;
+}
+
+ctb_status ctb_filter_kernel_ms(ctb_ctx* ctx, int back, double* ms) {
+    if (!ctx || !ms || back < 0 || back >= ctb_ctx::kProfRing || back >= ctx->prof_calls ||
+        ctx->prof_ev.empty())
+        return fail(ctx, CTB_ERR_INVALID, "ctb_filter_kernel_ms: no such profiled call");
+    Guard g(ctx);
+    const long long idx = (ctx->prof_calls - 1 - back) % ctb_ctx::kProfRing;
+    cudaEvent_t* ev = &ctx->prof_ev[idx * ctb_ctx::kProfEvents];
+    CTB_CUDA(ctx, cudaEventSynchronize(ev[4]));
+    float t = 0.f;
+    CTB_CUDA(ctx, cudaEventElapsedTime(&t, ev[5], ev[3]));
+    *ms = t;
     return CTB_OK;
 }
 

@@ -117,6 +117,10 @@ cudaError_t make_gemm_table(const PadGeom& g, int type, GemmTable* out);
 int gemm_kpad(int bins);
 // Device bytes of the BF16 row split the tensor-core filter needs.
 size_t filter_gemm_split_bytes(int nz, int na, int bins);
+// Operand split (two BF16 terms of every row) and the zero guard bins; then
+// the tensor-core product itself.
+cudaError_t launch_filter_gemm_prep(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
+                                    const GemmTable& tab, float4* d_filt, void* d_split, cudaStream_t st);
 cudaError_t launch_filter_gemm(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
                                const GemmTable& tab, const float4* d_stats, int denorm, float scale,
                                float4* d_filt, void* d_split, unsigned* d_err, cudaStream_t st);
@@ -223,7 +227,9 @@ struct ctb_ctx {
 
     // Stage profiling: a ring of event sets, one set per volume reconstruction.
     static constexpr int kProfRing = 256;
-    static constexpr int kProfEvents = 5;
+    // events 0..4 bracket the stages; event 5 marks the start of the filter's
+    // main kernel (after the tensor-core path's operand split)
+    static constexpr int kProfEvents = 6;
     bool profiling = false;
     std::vector<cudaEvent_t> prof_ev;  // kProfRing * kProfEvents
     long long prof_calls = 0;

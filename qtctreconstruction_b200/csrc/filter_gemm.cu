@@ -386,13 +386,12 @@ cudaError_t make_gemm_table(const PadGeom& g, int type, GemmTable* out) {
     return cudaSuccess;
 }
 
-cudaError_t launch_filter_gemm(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
-                               const GemmTable& tab, const float4* d_stats, int denorm, float scale,
-                               float4* d_filt, void* d_split, unsigned* d_err, cudaStream_t st) {
+cudaError_t launch_filter_gemm_prep(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
+                                    const GemmTable& tab, float4* d_filt, void* d_split, cudaStream_t st) {
     const int nzg = (nz + 3) / 4;
     const long long pairs = static_cast<long long>(nzg) * na;
     const long long rows = (pairs * 4 + BM - 1) / BM * BM;
-    if (rows / BM > 65535 || pairs > 0x7fffffffLL) return cudaErrorInvalidValue;
+    if (rows / BM > 65535) return cudaErrorInvalidValue;
     __nv_bfloat16* xh = static_cast<__nv_bfloat16*>(d_split);
     __nv_bfloat16* xl = xh + rows * tab.kpad;
     const long long items = rows * (tab.kpad / 8);
@@ -407,10 +406,21 @@ cudaError_t launch_filter_gemm(const float* d_sino, int nz, int na, const PadGeo
         if (e != cudaSuccess) return e;
     }
     const int right = fl.pitch - fl.guard - g.sq;
-    if (right > 0) {
-        e = cudaMemset2DAsync(d_filt + fl.guard + g.sq, pitch_b, 0, sizeof(float4) * right, pairs, st);
-        if (e != cudaSuccess) return e;
-    }
+    if (right > 0) e = cudaMemset2DAsync(d_filt + fl.guard + g.sq, pitch_b, 0, sizeof(float4) * right, pairs, st);
+    return e;
+}
+
+cudaError_t launch_filter_gemm(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
+                               const GemmTable& tab, const float4* d_stats, int denorm, float scale,
+                               float4* d_filt, void* d_split, unsigned* d_err, cudaStream_t st) {
+    const int nzg = (nz + 3) / 4;
+    const long long pairs = static_cast<long long>(nzg) * na;
+    const long long rows = (pairs * 4 + BM - 1) / BM * BM;
+    if (rows / BM > 65535 || pairs > 0x7fffffffLL) return cudaErrorInvalidValue;
+    (void)d_sino;
+    const __nv_bfloat16* xh = static_cast<const __nv_bfloat16*>(d_split);
+    const __nv_bfloat16* xl = xh + rows * tab.kpad;
+    cudaError_t e;
     CUtensorMap mxh, mxl, mth, mtl;
     if (!encode_map(&mxh, xh, rows, tab.kpad, BM) || !encode_map(&mxl, xl, rows, tab.kpad, BM))
         return cudaErrorNotSupported;
