@@ -11,7 +11,7 @@ data (no dataset involved); the volume (0.54 GB) exceeds the 126 MB L2, so no
 flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config small|large|medium|precision|batch|serving]
+                  [--config small|large|medium|precision|tcprof|batch|serving]
 
 N > 1 runs under torch.distributed.run, one rank per GPU, each rank
 reconstructing its own volume (weak scaling; no data-path collective).
@@ -42,6 +42,8 @@ CONFIGS = {
                    name="384^3 phantom (24 ellipsoids), 540 angles, Shepp-Logan (profiling size)"),
     "precision": dict(n=1024, nz=256, na=1440, ellipsoids=64, filter=4, seed=3,
                       name="1024^2 x 256 phantom (64 ellipsoids), 1440 angles, Hann"),
+    "tcprof": dict(n=1024, nz=16, na=1440, ellipsoids=64, filter=4, seed=3,
+                   name="1024^2 x 16 slices, 1440 angles, Hann (profiling size of the filter kernels)"),
     "batch": dict(jobs=64, seed=4,
                   name="64 uneven FBP jobs: N in {64..768}, 16-256 slices, round(pi/2 N) angles, "
                        "Ram-Lak/Shepp-Logan/Hann, sinograms of seeded 10-ellipsoid phantoms"),
