@@ -159,6 +159,24 @@ def measured_peaks():
         return {}
 
 
+# ------------------------------------------------------------------ ranks
+def max_over_ranks(dist, values, device):
+    """Element-wise maximum of per-rank timings; every rank calls it at the
+    same point (a no-op without a process group)."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def replica_throughput(world: int, units_per_rank: float, ms: float) -> float:
+    """Whole-job rate of `world` replicas, each processing `units_per_rank`
+    in at most `ms` (the max over ranks)."""
+    return world * units_per_rank / (ms * 1e-3)
+
+
 # ------------------------------------------------------------- CPU baseline
 def cpu_reference_rate(cfg: dict, slices: int, params, repeats: int = 1):
     """The reference's OpenMPBackend per-slice path (computeSinogram with the
@@ -310,14 +328,10 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
     barrier()
     e2e_ms = e2.elapsed_time(e3) / e2e_steps
 
-    # max over ranks
-    if dist is not None:
-        t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms], "cuda")
 
     if rank == 0:
-        value = world * updates / (ms * 1e-3)
+        value = replica_throughput(world, updates, ms)
         smem_gbs = be.probe_smem_bandwidth()
         inside = circle_voxels(n) * nz * na
         bp_ms = float(stages[3])
@@ -351,7 +365,7 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
                                 "peak": hbm_peak, "unit": "GB/s",
                                 "frac": (filt_bytes / (filt_kernel_ms * 1e-3) / 1e9 / hbm_peak) if hbm_peak else None,
                                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_peak else None},
-            "e2e": {"value": world * updates / (e2e_ms * 1e-3), "unit": UNIT,
+            "e2e": {"value": replica_throughput(world, updates, e2e_ms), "unit": UNIT,
                     "h2d_bytes_per_step": 4 * n * n * nz, "d2h_bytes_per_step": 4 * n * n * nz,
                     "ms_per_step": e2e_ms, "api": "ctb_reconstruct_volume (pinned host buffers)"},
             "clocks": clocks,
@@ -691,7 +705,9 @@ def main():
         args.filter_modes = True
     if args.config in ("batch", "serving"):
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": f"the reference has no {args.config} entry point"}))
+            if rank == 0:
+                print(json.dumps({"impl": "reference",
+                                  "unavailable": f"the reference has no {args.config} entry point"}))
             return 0
         run = run_batch if args.config == "batch" else run_serving
         return run(args, cfg, rank, world, local) if rank == 0 else 0
