@@ -334,6 +334,27 @@ ctb_status ctb_arena_free(ctb_arena* a, size_t offset);                  /* CTB_
 ctb_status ctb_arena_stats(const ctb_arena* a, size_t* used, size_t* peak, size_t* largest_free);
 void ctb_arena_destroy(ctb_arena* a);
 
+/* ------------------------------------------------------- sinogram files */
+
+/* The consumer format of the reference: sinograms as an NPY array
+ * (depth, num_angles, bins) of little-endian float32 plus a sidecar
+ * "<name>.meta.json" {version, depth, num_angles, detector_bins,
+ * detector_spacing_mm, original_min_hu, original_max_hu, angles_deg}
+ * (CtReconstructionController.cpp:1353-1482 export, :1494-1616 import; NPY
+ * layout FileIO.cpp:53-148). Host-only, no device calls.
+ *
+ * ctb_sinogram_file_shape reads the NPY header (versions 1-3, '<f4', C order,
+ * three dimensions) without the data. ctb_load_sinogram_file reads the data
+ * into sinos (depth * num_angles * bins floats) and, when non-NULL, the angles
+ * (num_angles floats: the sidecar's when their count is num_angles, else
+ * uniform 180/na * a) and meta[3] = {detector_spacing_mm (default 1),
+ * min, max (the sidecar's, else computed from the data)}.
+ * ctb_save_sinogram_file writes both files (angles NULL = uniform). */
+ctb_status ctb_sinogram_file_shape(const char* path, int* depth, int* num_angles, int* bins);
+ctb_status ctb_load_sinogram_file(const char* path, float* sinos, float* angles_deg, float* meta);
+ctb_status ctb_save_sinogram_file(const char* path, const float* sinos, int depth, int num_angles, int bins,
+                                  const float* angles_deg, float spacing_mm, float min_hu, float max_hu);
+
 /* ------------------------------------------------------------ phantoms */
 
 /* Summed random-ellipsoid phantom (the benchmark phantom; a new generator mode

@@ -155,6 +155,9 @@ def _declare(L):
     L.ctb_extract_point_cloud.argtypes = [p, p, i, i, i, f, p, ctypes.c_int64, P(ctypes.c_int64)]
     L.ctb_set_profiling.argtypes = [p, i]
     L.ctb_set_filter_mode.argtypes = [p, i]
+    L.ctb_sinogram_file_shape.argtypes = [ctypes.c_char_p, P(i), P(i), P(i)]
+    L.ctb_load_sinogram_file.argtypes = [ctypes.c_char_p, p, p, p]
+    L.ctb_save_sinogram_file.argtypes = [ctypes.c_char_p, p, i, i, i, p, f, f, f]
     L.ctb_filter_kernel_ms.argtypes = [p, i, P(ctypes.c_double)]
     L.ctb_stage_times.argtypes = [p, i, P(ctypes.c_double)]
     L.ctb_probe_smem_bandwidth.argtypes = [p, P(ctypes.c_double)]
@@ -229,6 +232,42 @@ def _ptr(a: np.ndarray):
 
 def _f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ------------------------------------------------------------ sinogram files
+def load_sinogram_file(path: str):
+    """Read a sinogram stack written in the reference's consumer format
+    (NPY (depth, num_angles, bins) float32 + optional <name>.meta.json):
+    returns (sinos, angles_deg, {"detector_spacing_mm", "original_min_hu",
+    "original_max_hu"}) with the reference's fallbacks for missing keys."""
+    L = library()
+    d, a, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    st = L.ctb_sinogram_file_shape(os.fsencode(path), ctypes.byref(d), ctypes.byref(a), ctypes.byref(b))
+    if st:
+        raise CtbError(st, f"cannot read {path}")
+    sinos = np.empty((d.value, a.value, b.value), np.float32)
+    ang = np.empty(a.value, np.float32)
+    meta = np.empty(3, np.float32)
+    st = L.ctb_load_sinogram_file(os.fsencode(path), sinos.ctypes.data, ang.ctypes.data, meta.ctypes.data)
+    if st:
+        raise CtbError(st, f"cannot read {path}")
+    return sinos, ang, {"detector_spacing_mm": float(meta[0]), "original_min_hu": float(meta[1]),
+                        "original_max_hu": float(meta[2])}
+
+
+def save_sinogram_file(path: str, sinos, angles_deg=None, spacing_mm: float = 1.0, min_hu=None, max_hu=None):
+    """Write sinograms[depth][num_angles][bins] in the consumer format (min/max
+    default to the data's)."""
+    s = _f32(sinos)
+    if s.ndim != 3:
+        raise ValueError("sinograms must be (depth, num_angles, bins)")
+    ang = None if angles_deg is None else _f32(angles_deg)
+    lo = float(s.min()) if min_hu is None else float(min_hu)
+    hi = float(s.max()) if max_hu is None else float(max_hu)
+    st = library().ctb_save_sinogram_file(os.fsencode(path), s.ctypes.data, *s.shape,
+                                          None if ang is None else ang.ctypes.data, spacing_mm, lo, hi)
+    if st:
+        raise CtbError(st, f"cannot write {path}")
 
 
 # ----------------------------------------------------------------- backend
@@ -671,6 +710,6 @@ GENERATOR3D_TISSUE = np.array(
     [-20.0, 45.0, 3.0, 10.0, 0.0, 0.0, 0.0, 1.0,
      200.0, 1000.0, 2.0, 8.0, 1.0, 0.7, 0.9, 0.15], dtype=np.float32)
 
-__all__ = ["FILTER_MODE_FFT", "FILTER_MODE_TC_BF16X3", "B200Backend", "Batch", "Server", "Arena", "ServerConfig", "Request", "ServerStats", "REQ_DEVICE", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
+__all__ = ["load_sinogram_file", "save_sinogram_file", "FILTER_MODE_FFT", "FILTER_MODE_TC_BF16X3", "B200Backend", "Batch", "Server", "Arena", "ServerConfig", "Request", "ServerStats", "REQ_DEVICE", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
            "library", "pad_geometry", "filter_response", "uniform_angles_deg", "odd_detector_count",
            "phantom_params", "GENERATOR3D_TISSUE", "LIB_PATH"]

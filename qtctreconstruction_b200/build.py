@@ -67,7 +67,27 @@ def build(verbose: bool = False, force: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    build_cli(verbose)
     return LIB
+
+
+CLI_SRC = os.path.join(PKG, "cli", "ctbench.cpp")
+CLI = os.path.join(PKG, "bin", "ctbench")
+
+
+def build_cli(verbose: bool = False) -> str:
+    """The headless C++ bench CLI, linked against libctb200.so (rpath $ORIGIN/..)."""
+    os.makedirs(os.path.dirname(CLI), exist_ok=True)
+    if os.path.exists(CLI) and os.path.getmtime(CLI) >= max(os.path.getmtime(CLI_SRC), os.path.getmtime(LIB)):
+        return CLI
+    cmd = [NVCC, "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"), CLI_SRC, "-o", CLI,
+           "-L" + PKG, "-lctb200", "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/..", "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"ctbench build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    if verbose and (r.stdout or r.stderr):
+        print(r.stdout + r.stderr, file=sys.stderr)
+    return CLI
 
 
 if __name__ == "__main__":

@@ -87,3 +87,12 @@ def test_create_without_gpu_reports_no_device():
     assert lib.ctb_create(ctypes.byref(h), 0) == 5  # CTB_ERR_NO_DEVICE
     with pytest.raises(ctb.CtbError):
         ctb.B200Backend(0)
+
+
+def test_cli_built_and_prints_usage():
+    """The headless C++ CLI (qtctreconstruction_b200/bin/ctbench) links against the library."""
+    import subprocess
+    cli = os.path.join(ROOT, "qtctreconstruction_b200", "bin", "ctbench")
+    assert os.path.exists(cli)
+    r = subprocess.run([cli], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "usage" in r.stderr
