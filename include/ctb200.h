@@ -113,6 +113,28 @@ ctb_status ctb_filter_kernel_ms(ctb_ctx* ctx, int back, double* ms);
 enum { CTB_FILTER_MODE_FFT = 0, CTB_FILTER_MODE_TC_BF16X3 = 1 };
 ctb_status ctb_set_filter_mode(ctb_ctx* ctx, int mode);
 
+/* Backprojection tile shapes. Four are compiled: 0 = 32x32 voxels, 4 per
+ * thread (the general case); 1 = 64x32, 8 per thread; 2 = 32x16, 2 per
+ * thread; 3 = 16x16, 1 per thread; all with 32 angles per staged chunk.
+ * Without tuning a job gets a shape from its size alone (32x32 once its
+ * tiles x slice groups reach the SM count, 32x16 above a quarter of it, else
+ * 16x16). With the autotuner
+ * on, the first job of each size bucket {ceil(n / 64), ceil(angles / 180),
+ * floor(log2(ceil(depth / 4)))} times every shape on its own data (that call
+ * synchronises) and the fastest is kept for the bucket; batches use a tuned
+ * shape when their job's bucket is tuned, else the default, so a job's shape
+ * never depends on the rest of a batch. The tuned table can be read and
+ * loaded as int quadruples {n bucket, angle bucket, depth bucket, shape}.
+ * Shapes differ in rounding only (all within the parity tolerance); no
+ * counterpart in the reference. */
+ctb_status ctb_set_bp_shape(ctb_ctx* ctx, int variant);  /* force a shape; -1 = automatic */
+ctb_status ctb_bp_shape_info(int variant, int* tile_x, int* tile_y, int* voxels_per_thread,
+                             int* angles_per_chunk);
+ctb_status ctb_bp_shape_for(ctb_ctx* ctx, int output_size, int depth, int num_angles, int* variant);
+ctb_status ctb_set_autotune(ctb_ctx* ctx, int enable);
+ctb_status ctb_autotune_table(ctb_ctx* ctx, int* entries, int capacity, int* count);
+ctb_status ctb_autotune_load(ctb_ctx* ctx, const int* entries, int count);
+
 /* Measured shared-memory load bandwidth of this GPU in GB/s: a conflict-free
  * 16-byte-per-lane load loop over all SMs, timed with CUDA events. The
  * backprojector's roofline denominator. */

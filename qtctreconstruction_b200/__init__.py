@@ -155,6 +155,12 @@ def _declare(L):
     L.ctb_extract_point_cloud.argtypes = [p, p, i, i, i, f, p, ctypes.c_int64, P(ctypes.c_int64)]
     L.ctb_set_profiling.argtypes = [p, i]
     L.ctb_set_filter_mode.argtypes = [p, i]
+    L.ctb_set_bp_shape.argtypes = [p, i]
+    L.ctb_bp_shape_info.argtypes = [i, P(i), P(i), P(i), P(i)]
+    L.ctb_bp_shape_for.argtypes = [p, i, i, i, P(i)]
+    L.ctb_set_autotune.argtypes = [p, i]
+    L.ctb_autotune_table.argtypes = [p, P(i), i, P(i)]
+    L.ctb_autotune_load.argtypes = [p, P(i), i]
     L.ctb_sinogram_file_shape.argtypes = [ctypes.c_char_p, P(i), P(i), P(i)]
     L.ctb_load_sinogram_file.argtypes = [ctypes.c_char_p, p, p, p]
     L.ctb_save_sinogram_file.argtypes = [ctypes.c_char_p, p, i, i, i, p, f, f, f]
@@ -187,6 +193,15 @@ def _declare(L):
 
 
 # ----------------------------------------------------------------- helpers
+def bp_shape_info(variant: int):
+    """(tile_x, tile_y, voxels_per_thread, angles_per_chunk) of a backprojection tile shape."""
+    v = [ctypes.c_int() for _ in range(4)]
+    st = library().ctb_bp_shape_info(variant, *[ctypes.byref(x) for x in v])
+    if st:
+        raise CtbError(st, "bp_shape_info")
+    return tuple(x.value for x in v)
+
+
 def pad_geometry(bins: int):
     """(square_bins, pad_before, fft_size) of reconstructSlice (SerialBackend.cpp:152-163)."""
     sq, pad, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
@@ -463,6 +478,32 @@ class B200Backend:
         """FILTER_MODE_FFT (default) or FILTER_MODE_TC_BF16X3 (tensor-core Toeplitz product)."""
         self._check(self._lib.ctb_set_filter_mode(self._h, int(mode)), "set_filter_mode")
 
+    def set_bp_shape(self, variant: int):
+        """Force a backprojection tile shape (0..3, see bp_shape_info); -1 = automatic."""
+        self._check(self._lib.ctb_set_bp_shape(self._h, int(variant)), "set_bp_shape")
+
+    def bp_shape_for(self, output_size: int, depth: int, num_angles: int) -> int:
+        v = ctypes.c_int()
+        self._check(self._lib.ctb_bp_shape_for(self._h, output_size, depth, num_angles, ctypes.byref(v)),
+                    "bp_shape_for")
+        return v.value
+
+    def set_autotune(self, enable: bool = True):
+        self._check(self._lib.ctb_set_autotune(self._h, int(bool(enable))), "set_autotune")
+
+    def autotune_table(self):
+        """[(n bucket, angle bucket, depth bucket, shape), ...] of the tuned buckets."""
+        n = ctypes.c_int()
+        self._check(self._lib.ctb_autotune_table(self._h, None, 0, ctypes.byref(n)), "autotune_table")
+        buf = (ctypes.c_int * (4 * max(n.value, 1)))()
+        self._check(self._lib.ctb_autotune_table(self._h, buf, n.value, ctypes.byref(n)), "autotune_table")
+        return [tuple(buf[4 * k:4 * k + 4]) for k in range(n.value)]
+
+    def autotune_load(self, entries):
+        flat = [int(x) for e in entries for x in e]
+        buf = (ctypes.c_int * max(len(flat), 1))(*flat)
+        self._check(self._lib.ctb_autotune_load(self._h, buf, len(flat) // 4), "autotune_load")
+
     def set_profiling(self, enable: bool = True):
         self._check(self._lib.ctb_set_profiling(self._h, int(bool(enable))), "set_profiling")
 
@@ -710,6 +751,6 @@ GENERATOR3D_TISSUE = np.array(
     [-20.0, 45.0, 3.0, 10.0, 0.0, 0.0, 0.0, 1.0,
      200.0, 1000.0, 2.0, 8.0, 1.0, 0.7, 0.9, 0.15], dtype=np.float32)
 
-__all__ = ["load_sinogram_file", "save_sinogram_file", "FILTER_MODE_FFT", "FILTER_MODE_TC_BF16X3", "B200Backend", "Batch", "Server", "Arena", "ServerConfig", "Request", "ServerStats", "REQ_DEVICE", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
+__all__ = ["bp_shape_info", "load_sinogram_file", "save_sinogram_file", "FILTER_MODE_FFT", "FILTER_MODE_TC_BF16X3", "B200Backend", "Batch", "Server", "Arena", "ServerConfig", "Request", "ServerStats", "REQ_DEVICE", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
            "library", "pad_geometry", "filter_response", "uniform_angles_deg", "odd_detector_count",
            "phantom_params", "GENERATOR3D_TISSUE", "LIB_PATH"]

@@ -82,5 +82,11 @@ ctb_status filter_tables(ctb_ctx* ctx, const PadGeom& g, int type, const float2*
                          const float2** d_tw);
 // Reads and clears the device error word (synchronises the context's stream).
 ctb_status check_error_word(ctb_ctx* ctx);
+// Autotuner bucket of a backprojection job: {ceil(n / 64), ceil(na / 180),
+// floor(log2(slice groups))}.
+std::vector<int> bp_bucket(int n_out, int nz, int na);
+// The tile shape a context uses for a job without timing anything: forced,
+// tuned for the job's bucket, or the default.
+int bp_variant_for(const ctb_ctx* ctx, int n_out, int nz, int na);
 
 }  // namespace ctb

@@ -10,21 +10,25 @@
 // reconstruction, denormalised with the slice's span and minimum (span folded
 // into the filter output, minimum added in the epilogue).
 //
-// Work decomposition: a work item is a 32 x 32 voxel tile of four slices (the
+// Work decomposition: a work item is a TX x TY voxel tile of four slices (the
 // float4 lanes of the filtered rows) of one job. Per angle, the detector window
-// that the tile can touch (kBpWindow bins) is staged into shared memory by the
-// bulk-copy engine (cp.async.bulk, completion on an mbarrier), 32 angles per
+// that the tile can touch (WIN bins) is staged into shared memory by the
+// bulk-copy engine (cp.async.bulk, completion on an mbarrier), CA angles per
 // chunk, double-buffered. The tile origin's detector coordinate is evaluated in
 // double precision once per angle and split into the window start and a
 // fractional offset, so each thread evaluates u in float on small numbers
-// (|u_local| < 48): the interpolation position is ~10x more accurate than the
-// reference's float u of magnitude ~sq. Each thread accumulates 4 voxels x 4
-// slices in registers; voxels outside the circle load nothing.
+// (|u_local| < WIN): the interpolation position is ~10x more accurate than the
+// reference's float u of magnitude ~sq. Each of the 256 threads accumulates
+// VPT voxels x 4 slices in registers; voxels outside the circle load nothing.
+// Four tile shapes are compiled (32x32 / 4 per thread, the default; 64x32 / 8;
+// 32x16 / 2; 16x16 / 1); bp_default_variant picks one from the job's size, the
+// context's autotuner can time them per size bucket.
 //
 // One kernel serves both shapes of work: a single job with one CTA per item,
 // or a batch of jobs (BpBatch) on a persistent grid that takes items from an
-// atomic counter. An item's arithmetic does not depend on the batch, so a
-// job's output is bit-identical alone and in any mix.
+// atomic counter. An item's arithmetic depends only on its job and tile shape,
+// so a job's output is bit-identical alone and in any mix of the same shape.
+#include <algorithm>
 #include <cmath>
 
 #include "ctb_internal.h"
@@ -32,13 +36,28 @@
 namespace ctb {
 namespace {
 
-constexpr int TILE = kBpTile;
-constexpr int WIN = kBpWindow;
-constexpr int CA = 32;        // angles per chunk
 constexpr int NBUF = 2;       // chunk buffers
-constexpr int THREADS = 256;  // 8 (x) x 32 (y) threads, 4 x-positions each
+constexpr int THREADS = 256;
 constexpr float kRound = 12582912.0f;   // 1.5 * 2^23: x + kRound rounds x to an integer
 constexpr int kRoundBits = 0x4B400000;  // bit pattern of kRound
+
+// A tile shape: TX x TY voxels of four slices, VPT voxels per thread along x
+// (spaced XS = TX / VPT apart), CA angles per staged chunk and WIN bins per
+// staged window (>= ceil(sqrt((TX-1)^2 + (TY-1)^2)) + 3 plus rounding margin:
+// the taps of every tile position lie in [ws, ws + span + 3)). MINB is the
+// launch-bounds occupancy target (registers 65536 / (256 MINB)).
+template <int TX_, int TY_, int VPT_, int CA_, int WIN_, int MINB_>
+struct Shape {
+    static constexpr int TX = TX_, TY = TY_, VPT = VPT_, CA = CA_, WIN = WIN_, MINB = MINB_;
+    static constexpr int XS = TX / VPT;
+    static_assert(XS * TY == THREADS, "256 threads per CTA");
+    static_assert(CA <= THREADS, "one thread per staged angle");
+    static_assert(WIN <= kBpWindowMax, "window within the filtered-row guard");
+};
+using V0 = Shape<32, 32, 4, 32, 52, 4>;  // the general-purpose shape
+using V1 = Shape<64, 32, 8, 32, 76, 2>;  // wide tiles: half the staging per voxel
+using V2 = Shape<32, 16, 2, 32, 40, 4>;  // half-height tiles: twice the CTAs
+using V3 = Shape<16, 16, 1, 32, 28, 4>;  // small tiles for small slices
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -88,19 +107,22 @@ struct AngleRec {
     int pad;
 };
 
+template <class C>
 struct BpSmem {
-    float4 win[NBUF][CA][WIN];
-    AngleRec rec[NBUF][CA];
+    float4 win[NBUF][C::CA][C::WIN];
+    AngleRec rec[NBUF][C::CA];
     unsigned long long bar[NBUF];
 };
 
 // Backproject one tile (x0, y0) of slice group zg of job J. `chunks` counts
 // the chunks this CTA has consumed so far (mbarrier phases continue across
 // items). Returns false when a bounded wait gave up (block-uniform).
-__device__ __forceinline__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x0, int y0, unsigned& chunks,
-                        unsigned* err) {
+template <class C>
+__device__ __forceinline__ bool bp_tile(BpSmem<C>& S, const BpJob& J, int zg, int x0, int y0, unsigned& chunks,
+                                        unsigned* err) {
+    constexpr int TX = C::TX, TY = C::TY, VPT = C::VPT, XS = C::XS, CA = C::CA, WIN = C::WIN;
     const int t = threadIdx.x;
-    const int lx = t & 7, ly = t >> 3;
+    const int lx = t % XS, ly = t / XS;
     const int n = J.n, nz = J.nz, na = J.na, sq = J.sq;
     const int rad = n / 2;
     const float radf = static_cast<float>(rad);
@@ -114,14 +136,14 @@ __device__ __forceinline__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x
 
     // Tiles entirely outside the reconstruction circle hold only the offset.
     {
-        const int xe = min(x0 + TILE - 1, n - 1), ye = min(y0 + TILE - 1, n - 1);
+        const int xe = min(x0 + TX - 1, n - 1), ye = min(y0 + TY - 1, n - 1);
         const long long dx = max(0, max(x0 - rad, rad - xe));
         const long long dy = max(0, max(y0 - rad, rad - ye));
         if (dx * dx + dy * dy > static_cast<long long>(rad) * rad) {
             const int y = y0 + ly;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int x = x0 + lx + 8 * k;
+            for (int k = 0; k < VPT; ++k) {
+                const int x = x0 + lx + XS * k;
                 if (x >= n || y >= n) continue;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
@@ -147,8 +169,8 @@ __device__ __forceinline__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x
             const double2 tc = J.trig.cs[a];
             const float2 tf = J.trig.csf[a];
             const double uo = ox * tc.x - oy * tc.y + dcd;
-            const double umin = uo + fmin(0.0, (TILE - 1) * tc.x) + fmin(0.0, -(TILE - 1) * tc.y);
-            const double umax = uo + fmax(0.0, (TILE - 1) * tc.x) + fmax(0.0, -(TILE - 1) * tc.y);
+            const double umin = uo + fmin(0.0, (TX - 1) * tc.x) + fmin(0.0, -(TY - 1) * tc.y);
+            const double umax = uo + fmax(0.0, (TX - 1) * tc.x) + fmax(0.0, -(TY - 1) * tc.y);
             const int ws = static_cast<int>(floor(umin)) - 1;
             AngleRec r;
             r.f0 = static_cast<float>(uo - ws);
@@ -167,9 +189,9 @@ __device__ __forceinline__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x
         if (t == 0) mbar_expect_tx(&S.bar[b], static_cast<unsigned>(cnt * WIN * sizeof(float4)));
     };
 
-    float4 acc[4];
+    float4 acc[VPT];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = 0; k < VPT; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
     const float fx = static_cast<float>(lx), fy = static_cast<float>(ly);
     // positions inside the reconstruction circle (SerialBackend.cpp:220-224);
     // the others are written as the offset only, so their taps are never loaded
@@ -177,8 +199,8 @@ __device__ __forceinline__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x
     {
         const float yy = static_cast<float>(y0 + ly) - radf;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const float xx = static_cast<float>(x0 + lx + 8 * k) - radf;
+        for (int k = 0; k < VPT; ++k) {
+            const float xx = static_cast<float>(x0 + lx + XS * k) - radf;
             if (!(xx * xx + yy * yy > radf * radf)) inside_mask |= 1u << k;
         }
     }
@@ -198,14 +220,14 @@ __device__ __forceinline__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x
             const AngleRec r = S.rec[b][j];
             const float4* w = S.win[b][j];
             const float ub = fmaf(fx, r.c, fmaf(-fy, r.s, r.f0));
-            const float c8 = 8.0f * r.c;
+            const float c8 = static_cast<float>(XS) * r.c;
             if (!r.edge) {
                 // i = floor(u) by rounding u - 1/2 with the kRound addition (no
                 // conversion-unit instructions); at an exact tie u = i + 1 the taps
                 // shift to (i, i+1) with weights (0, 1), the same value
                 const float ubh = ub - 0.5f;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < VPT; ++k) {
                     if (!(inside_mask & (1u << k))) continue;
                     const float uh = fmaf(static_cast<float>(k), c8, ubh);
                     const float tr = uh + kRound;
@@ -225,12 +247,12 @@ __device__ __forceinline__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x
                 // 0 <= floor(u) and floor(u) + 1 < sq; that decision is reproduced
                 // here exactly, the interpolation itself uses the accurate u.
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < VPT; ++k) {
                     if (!(inside_mask & (1u << k))) continue;
                     const float u = fmaf(static_cast<float>(k), c8, ub);
                     const float fl = floorf(u);
                     const int i = static_cast<int>(fl);
-                    const float xs = static_cast<float>(x0 + lx + 8 * k - rad);
+                    const float xs = static_cast<float>(x0 + lx + XS * k - rad);
                     const float ys = static_cast<float>(y0 + ly - rad);
                     const float us = __fadd_rn(__fsub_rn(__fmul_rn(xs, r.cf), __fmul_rn(ys, r.sf)), dcf);
                     const int is = static_cast<int>(floorf(us));
@@ -251,8 +273,8 @@ __device__ __forceinline__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x
 
     const int y = y0 + ly;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int x = x0 + lx + 8 * k;
+    for (int k = 0; k < VPT; ++k) {
+        const int x = x0 + lx + XS * k;
         if (x >= n || y >= n) continue;
         const bool inside = inside_mask & (1u << k);
         const float v[4] = {acc[k].x, acc[k].y, acc[k].z, acc[k].w};
@@ -267,12 +289,12 @@ __device__ __forceinline__ bool bp_tile(BpSmem& S, const BpJob& J, int zg, int x
 
 // PERSISTENT = false: one CTA per item (item = blockIdx.x). Otherwise a
 // persistent grid whose thread 0 draws items from *counter.
-template <bool PERSISTENT>
-__global__ void __launch_bounds__(THREADS, 4) k_backproject(const __grid_constant__ BpBatch batch,
-                                                            unsigned* __restrict__ counter,
-                                                            unsigned* __restrict__ err) {
+template <class C, bool PERSISTENT>
+__global__ void __launch_bounds__(THREADS, C::MINB) k_backproject(const __grid_constant__ BpBatch batch,
+                                                                  unsigned* __restrict__ counter,
+                                                                  unsigned* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    BpSmem& S = *reinterpret_cast<BpSmem*>(smem_raw);
+    BpSmem<C>& S = *reinterpret_cast<BpSmem<C>*>(smem_raw);
     __shared__ int s_item;
     if (threadIdx.x == 0) {
         for (int b = 0; b < NBUF; ++b) mbar_init(&S.bar[b], 1);
@@ -286,7 +308,7 @@ __global__ void __launch_bounds__(THREADS, 4) k_backproject(const __grid_constan
         const BpJob& J = batch.job[0];
         const int zg = blockIdx.x / J.tiles;
         const int tl = blockIdx.x - zg * J.tiles;
-        bp_tile(S, J, zg, (tl % J.tiles_x) * TILE, (tl / J.tiles_x) * TILE, chunks, err);
+        bp_tile<C>(S, J, zg, (tl % J.tiles_x) * C::TX, (tl / J.tiles_x) * C::TY, chunks, err);
         return;
     }
     for (;;) {
@@ -300,44 +322,93 @@ __global__ void __launch_bounds__(THREADS, 4) k_backproject(const __grid_constan
         const int local = item - static_cast<int>(J.first);
         const int zg = local / J.tiles;
         const int tl = local - zg * J.tiles;
-        if (!bp_tile(S, J, zg, (tl % J.tiles_x) * TILE, (tl / J.tiles_x) * TILE, chunks, err)) break;
+        if (!bp_tile<C>(S, J, zg, (tl % J.tiles_x) * C::TX, (tl / J.tiles_x) * C::TY, chunks, err)) break;
         __syncthreads();  // shared state of this item is dead before the next item's staging
     }
 }
 
-size_t bp_smem() { return sizeof(BpSmem); }
-
-cudaError_t set_bp_smem() {
-    cudaError_t e = cudaFuncSetAttribute(k_backproject<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(bp_smem()));
+template <class C>
+cudaError_t set_smem() {
+    cudaError_t e = cudaFuncSetAttribute(k_backproject<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(sizeof(BpSmem<C>)));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_backproject<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(bp_smem()));
+    return cudaFuncSetAttribute(k_backproject<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sizeof(BpSmem<C>)));
+}
+
+template <class C>
+cudaError_t launch_one(const BpBatch& b, unsigned* d_err, cudaStream_t st) {
+    cudaError_t e = set_smem<C>();
+    if (e != cudaSuccess) return e;
+    k_backproject<C, false><<<static_cast<unsigned>(b.total), THREADS, sizeof(BpSmem<C>), st>>>(b, nullptr, d_err);
+    return cudaGetLastError();
+}
+
+template <class C>
+cudaError_t launch_persistent(const BpBatch& b, unsigned* d_counter, unsigned* d_err, cudaStream_t st) {
+    cudaError_t e = set_smem<C>();
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backproject<C, true>, THREADS, sizeof(BpSmem<C>));
+    const long long grid = std::min<long long>(b.total, static_cast<long long>(sms) * (per_sm > 0 ? per_sm : 1));
+    e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    k_backproject<C, true><<<static_cast<unsigned>(grid), THREADS, sizeof(BpSmem<C>), st>>>(b, d_counter, d_err);
+    return cudaGetLastError();
+}
+
+template <class C>
+BpShape shape_of() {
+    return BpShape{C::TX, C::TY, C::VPT, C::CA, C::WIN};
 }
 
 }  // namespace
 
+BpShape bp_shape(int variant) {
+    switch (variant) {
+    case 1: return shape_of<V1>();
+    case 2: return shape_of<V2>();
+    case 3: return shape_of<V3>();
+    default: return shape_of<V0>();
+    }
+}
+
+int bp_default_variant(int n_out, int nz, int sms) {
+    // Measured on B200 (fbp of random sinograms, shapes forced): the 32x32
+    // tile is fastest once its CTAs reach the SM count (n >= 128 at 64
+    // slices); below that smaller tiles win by filling more SMs (n = 64,
+    // 16 slices: 16x16 0.025 ms, 32x16 0.031 ms, 32x32 0.044 ms). The 64x32
+    // tile never won and is left to the autotuner.
+    const long long ctas = static_cast<long long>((n_out + 31) / 32) * ((n_out + 31) / 32) * ((nz + 3) / 4);
+    if (ctas >= sms) return 0;
+    if (4 * ctas >= sms) return 2;
+    return 3;
+}
+
 FiltLayout filt_layout(int sq, int n_out) {
-    // Every position of the tile grid (n rounded up to whole tiles) lies within
-    // m = max(r, n_pad - 1 - r) of the centre along each axis, so |u - dc| <=
-    // m * sqrt(2); windows start one bin below the tile's minimum and span
-    // kBpWindow bins.
+    // Every position of every tile grid (n rounded up to whole tiles of any
+    // shape, at most kBpTileMax) lies within m = max(r, n_pad - 1 - r) of the
+    // centre along each axis, so |u - dc| <= m * sqrt(2); windows start one
+    // bin below the tile's minimum and span at most kBpWindowMax bins.
     FiltLayout fl;
     fl.sq = sq;
     const int r = n_out / 2;
-    const int n_pad = (n_out + kBpTile - 1) / kBpTile * kBpTile;
+    const int n_pad = (n_out + kBpTileMax - 1) / kBpTileMax * kBpTileMax;
     const int m = r > n_pad - 1 - r ? r : n_pad - 1 - r;
     const double reach = m * std::sqrt(2.0) + 3.0;
     const double dc = sq / 2;
     const int left = static_cast<int>(std::ceil(reach + 2.0 - dc));
-    const int right = static_cast<int>(std::ceil(dc + reach + kBpWindow + 2.0 - sq));
+    const int right = static_cast<int>(std::ceil(dc + reach + kBpWindowMax + 2.0 - sq));
     fl.guard = left > 0 ? left : 0;
     fl.pitch = fl.guard + sq + (right > 0 ? right : 0);
     return fl;
 }
 
 BpJob make_bp_job(const float4* d_filt, int nz, int na, const FiltLayout& fl, int n_out, Trig trig,
-                  const float4* d_stats, int denorm, float* d_out) {
+                  const float4* d_stats, int denorm, float* d_out, int variant) {
+    const BpShape sh = bp_shape(variant);
     BpJob J;
     J.filt = d_filt;
     J.out = d_out;
@@ -350,40 +421,38 @@ BpJob make_bp_job(const float4* d_filt, int nz, int na, const FiltLayout& fl, in
     J.pitch = fl.pitch;
     J.n = n_out;
     J.denorm = denorm;
-    J.tiles_x = (n_out + TILE - 1) / TILE;
-    J.tiles = J.tiles_x * J.tiles_x;
+    J.tiles_x = (n_out + sh.tx - 1) / sh.tx;
+    J.tiles = J.tiles_x * ((n_out + sh.ty - 1) / sh.ty);
     J.first = 0;
     return J;
 }
 
-cudaError_t launch_backproject_batch(const BpBatch& b, unsigned* d_counter, unsigned* d_err,
+cudaError_t launch_backproject_batch(const BpBatch& b, int variant, unsigned* d_counter, unsigned* d_err,
                                      cudaStream_t st) {
-    cudaError_t e = set_bp_smem();
-    if (e != cudaSuccess || b.total == 0) return e;
+    if (b.total == 0) return cudaSuccess;
     if (b.total > 0x7fffffffLL) return cudaErrorInvalidValue;
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backproject<true>, THREADS, bp_smem());
-    const long long grid = std::min<long long>(b.total, static_cast<long long>(sms) * (per_sm > 0 ? per_sm : 1));
-    e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned), st);
-    if (e != cudaSuccess) return e;
-    k_backproject<true><<<static_cast<unsigned>(grid), THREADS, bp_smem(), st>>>(b, d_counter, d_err);
-    return cudaGetLastError();
+    switch (variant) {
+    case 1: return launch_persistent<V1>(b, d_counter, d_err, st);
+    case 2: return launch_persistent<V2>(b, d_counter, d_err, st);
+    case 3: return launch_persistent<V3>(b, d_counter, d_err, st);
+    default: return launch_persistent<V0>(b, d_counter, d_err, st);
+    }
 }
 
 cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltLayout& fl,
                                int n_out, Trig trig, const float4* d_stats, int denorm,
-                               float* d_out, unsigned* d_err, cudaStream_t st) {
-    cudaError_t e = set_bp_smem();
-    if (e != cudaSuccess) return e;
+                               float* d_out, unsigned* d_err, cudaStream_t st, int variant) {
     BpBatch b;
     b.njobs = 1;
-    b.job[0] = make_bp_job(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out);
+    b.job[0] = make_bp_job(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out, variant);
     b.total = static_cast<long long>(b.job[0].tiles) * ((nz + 3) / 4);
     if (b.total > 0x7fffffffLL) return cudaErrorInvalidValue;
-    k_backproject<false><<<static_cast<unsigned>(b.total), THREADS, bp_smem(), st>>>(b, nullptr, d_err);
-    return cudaGetLastError();
+    switch (variant) {
+    case 1: return launch_one<V1>(b, d_err, st);
+    case 2: return launch_one<V2>(b, d_err, st);
+    case 3: return launch_one<V3>(b, d_err, st);
+    default: return launch_one<V0>(b, d_err, st);
+    }
 }
 
 }  // namespace ctb

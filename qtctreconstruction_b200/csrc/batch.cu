@@ -26,6 +26,7 @@ struct ctb_batch {
     std::vector<ctb_fbp_job> jobs;
     std::vector<FiltBatch> filt;  // one launch each
     std::vector<BpBatch> bp;      // one launch each
+    std::vector<int> bp_variant;  // tile shape of each backprojection launch
     void* mem = nullptr;          // angle tables + filtered rows of every job
     size_t bytes = 0;
     unsigned* d_counter = nullptr;
@@ -55,7 +56,9 @@ ctb_status check_job(ctb_ctx* ctx, const ctb_fbp_job& j, int i) {
 ctb_status issue(ctb_batch* b) {
     ctb_ctx* ctx = b->ctx;
     for (const FiltBatch& f : b->filt) CTB_LAUNCH(ctx, launch_filter_batch(f, ctx->stream));
-    for (const BpBatch& p : b->bp) {
+    for (size_t i = 0; i < b->bp.size(); ++i) {
+        const BpBatch& p = b->bp[i];
+        const int v = b->bp_variant[i];
         if (b->flags & CTB_BATCH_PER_JOB) {
             const BpJob& J = p.job[0];
             FiltLayout fl;
@@ -63,9 +66,9 @@ ctb_status issue(ctb_batch* b) {
             fl.guard = J.guard;
             fl.pitch = J.pitch;
             CTB_LAUNCH(ctx, launch_backproject(J.filt, J.nz, J.na, fl, J.n, J.trig, nullptr,
-                                               CTB_DENORM_NONE, J.out, ctx->d_err, ctx->stream));
+                                               CTB_DENORM_NONE, J.out, ctx->d_err, ctx->stream, v));
         } else {
-            CTB_LAUNCH(ctx, launch_backproject_batch(p, b->d_counter, ctx->d_err, ctx->stream));
+            CTB_LAUNCH(ctx, launch_backproject_batch(p, v, b->d_counter, ctx->d_err, ctx->stream));
         }
     }
     return CTB_OK;
@@ -109,6 +112,7 @@ ctb_status build(ctb_batch* b) {
 
     std::vector<FiltJob> fj(n);
     std::vector<BpJob> bj(n);
+    std::vector<int> var(n);
     for (int i = 0; i < n; ++i) {
         const ctb_fbp_job& j = b->jobs[i];
         const Geo& q = geo[i];
@@ -130,8 +134,10 @@ ctb_status build(ctb_batch* b) {
         float4* d_filt = reinterpret_cast<float4*>(base + q.filt_off);
         fj[i] = make_filt_job(j.sino, j.depth, j.num_angles, q.g, q.fl, d_Hc, nullptr, CTB_DENORM_NONE,
                               scale, d_filt);
+        // the shape fbp_d would use for this job alone (no timing here)
+        var[i] = bp_variant_for(ctx, j.output_size, j.depth, j.num_angles);
         bj[i] = make_bp_job(d_filt, j.depth, j.num_angles, q.fl, j.output_size, trig, nullptr,
-                            CTB_DENORM_NONE, j.out);
+                            CTB_DENORM_NONE, j.out, var[i]);
     }
 
     const bool per_job = (b->flags & CTB_BATCH_PER_JOB) != 0;
@@ -155,15 +161,18 @@ ctb_status build(ctb_batch* b) {
         }
         b->filt.push_back(f);
     }
-    // backprojection: most angles first (the most expensive items lead the queue)
+    // backprojection: one persistent launch per tile shape, most angles first
+    // (the most expensive items lead the queue)
     std::vector<int> by_na(n);
     std::iota(by_na.begin(), by_na.end(), 0);
-    std::stable_sort(by_na.begin(), by_na.end(),
-                     [&](int x, int y) { return b->jobs[x].num_angles > b->jobs[y].num_angles; });
+    std::stable_sort(by_na.begin(), by_na.end(), [&](int x, int y) {
+        return var[x] != var[y] ? var[x] < var[y] : b->jobs[x].num_angles > b->jobs[y].num_angles;
+    });
     if (per_job) std::iota(by_na.begin(), by_na.end(), 0);
     for (int k = 0; k < n;) {
         BpBatch p;
-        while (k < n && p.njobs < cap) {
+        const int v = var[by_na[k]];
+        while (k < n && p.njobs < cap && var[by_na[k]] == v) {
             BpJob J = bj[by_na[k]];
             J.first = p.total;
             p.total += static_cast<long long>(J.tiles) * ((J.nz + 3) / 4);
@@ -171,6 +180,7 @@ ctb_status build(ctb_batch* b) {
             ++k;
         }
         b->bp.push_back(p);
+        b->bp_variant.push_back(v);
     }
     b->kernel_launches = static_cast<int>(b->filt.size() + b->bp.size());
 

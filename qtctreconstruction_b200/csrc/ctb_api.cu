@@ -136,6 +136,21 @@ ctb_status filter_tables(ctb_ctx* ctx, const PadGeom& g, int type, const float2*
     return CTB_OK;
 }
 
+std::vector<int> bp_bucket(int n_out, int nz, int na) {
+    int zb = 0;
+    for (int zg = (nz + 3) / 4; zg > 1; zg >>= 1) ++zb;
+    return {(n_out + 63) / 64, (na + 179) / 180, zb};
+}
+
+int bp_variant_for(const ctb_ctx* ctx, int n_out, int nz, int na) {
+    if (ctx->bp_variant >= 0) return ctx->bp_variant;
+    if (ctx->autotune) {
+        auto it = ctx->tuned.find(bp_bucket(n_out, nz, na));
+        if (it != ctx->tuned.end()) return it->second;
+    }
+    return bp_default_variant(n_out, nz, ctx->sms);
+}
+
 ctb_status check_error_word(ctb_ctx* ctx) {
     unsigned h = 0;
     CTB_CUDA(ctx, cudaMemcpyAsync(&h, ctx->d_err, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
@@ -213,6 +228,47 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     return CTB_OK;
 }
 
+// First job of a size bucket with the autotuner on: time every tile shape on
+// this job's own filtered rows (two launches each, CUDA events, synchronous),
+// keep the fastest for the bucket. The caller then runs the chosen shape, so
+// the output is that shape's.
+ctb_status tune_backprojection(ctb_ctx* ctx, const float4* d_filt, int nz, int na, const FiltLayout& fl,
+                               int n_out, Trig trig, const float4* d_stats, int denorm, float* d_out,
+                               int* variant) {
+    cudaEvent_t e0, e1;
+    CTB_CUDA(ctx, cudaEventCreate(&e0));
+    CTB_CUDA(ctx, cudaEventCreate(&e1));
+    float best = 0.f;
+    int best_v = *variant;
+    for (int v = 0; v < kBpVariants; ++v) {
+        cudaError_t e = launch_backproject(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out, ctx->d_err,
+                                           ctx->stream, v);  // warm-up
+        if (e == cudaSuccess) e = cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < 2 && e == cudaSuccess; ++r)
+            e = launch_backproject(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out, ctx->d_err,
+                                   ctx->stream, v);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return fail(ctx, CTB_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+        }
+        ctx->launches += 3;
+        if (v == 0 || ms < best) {
+            best = ms;
+            best_v = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->tuned[bp_bucket(n_out, nz, na)] = best_v;
+    *variant = best_v;
+    return CTB_OK;
+}
+
 ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins,
                      const float* angles_deg, int n_out, int filter, const float4* d_stats,
                      int denorm, float* d_out, cudaEvent_t* ev = nullptr) {
@@ -249,8 +305,11 @@ ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins
                                       ctx->stream));
     }
     mark(ctx, ev, 3);
+    int variant = bp_variant_for(ctx, n_out, nz, na);
+    if (ctx->autotune && ctx->bp_variant < 0 && !ctx->tuned.count(bp_bucket(n_out, nz, na)))
+        CTB_TRY(tune_backprojection(ctx, d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out, &variant));
     CTB_LAUNCH(ctx, launch_backproject(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out,
-                                       ctx->d_err, ctx->stream));
+                                       ctx->d_err, ctx->stream, variant));
     return CTB_OK;
 }
 
@@ -304,6 +363,7 @@ ctb_status ctb_create(ctb_ctx** out, int device) {
     }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
     ctx->stream = ctx->own_stream;
+    ctx->sms = prop.multiProcessorCount;
     *out = ctx;
     return CTB_OK;
 }
@@ -366,6 +426,63 @@ ctb_status ctb_filter_response(int fft_size, int filter, float* H) {
     if (fft_size < 2 || (fft_size & (fft_size - 1)) || !H) return CTB_ERR_INVALID;
     const auto v = filter_response(fft_size, filter);
     for (size_t i = 0; i < v.size(); ++i) H[i] = static_cast<float>(v[i]);
+    return CTB_OK;
+}
+
+ctb_status ctb_set_bp_shape(ctb_ctx* ctx, int variant) {
+    if (!ctx || variant < -1 || variant >= kBpVariants) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    ctx->bp_variant = variant;
+    return CTB_OK;
+}
+
+ctb_status ctb_bp_shape_info(int variant, int* tile_x, int* tile_y, int* voxels_per_thread,
+                             int* angles_per_chunk) {
+    if (variant < 0 || variant >= kBpVariants) return CTB_ERR_INVALID;
+    const BpShape sh = bp_shape(variant);
+    if (tile_x) *tile_x = sh.tx;
+    if (tile_y) *tile_y = sh.ty;
+    if (voxels_per_thread) *voxels_per_thread = sh.vpt;
+    if (angles_per_chunk) *angles_per_chunk = sh.ca;
+    return CTB_OK;
+}
+
+ctb_status ctb_bp_shape_for(ctb_ctx* ctx, int output_size, int depth, int num_angles, int* variant) {
+    if (!ctx || !variant || output_size <= 0 || depth <= 0 || num_angles <= 0) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    *variant = bp_variant_for(ctx, output_size, depth, num_angles);
+    return CTB_OK;
+}
+
+ctb_status ctb_set_autotune(ctb_ctx* ctx, int enable) {
+    if (!ctx) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    ctx->autotune = enable != 0;
+    return CTB_OK;
+}
+
+ctb_status ctb_autotune_table(ctb_ctx* ctx, int* entries, int capacity, int* count) {
+    if (!ctx || !count || capacity < 0 || (capacity > 0 && !entries)) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    int k = 0;
+    for (const auto& kv : ctx->tuned) {
+        if (k < capacity) {
+            for (int i = 0; i < 3; ++i) entries[4 * k + i] = kv.first[i];
+            entries[4 * k + 3] = kv.second;
+        }
+        ++k;
+    }
+    *count = k;
+    return CTB_OK;
+}
+
+ctb_status ctb_autotune_load(ctb_ctx* ctx, const int* entries, int count) {
+    if (!ctx || count < 0 || (count > 0 && !entries)) return CTB_ERR_INVALID;
+    for (int k = 0; k < count; ++k)
+        if (entries[4 * k + 3] < 0 || entries[4 * k + 3] >= kBpVariants) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    for (int k = 0; k < count; ++k)
+        ctx->tuned[{entries[4 * k], entries[4 * k + 1], entries[4 * k + 2]}] = entries[4 * k + 3];
     return CTB_OK;
 }
 

@@ -44,9 +44,19 @@ struct FiltLayout {
     int guard = 0;
     int pitch = 0;
 };
-constexpr int kBpTile = 32;      // backprojection tile edge (voxels)
-constexpr int kBpWindow = 52;    // bins staged per angle and tile (>= 31*sqrt(2) + margins)
+constexpr int kBpTileMax = 64;     // widest backprojection tile edge (voxels)
+constexpr int kBpWindowMax = 76;   // most bins staged per angle and tile
 FiltLayout filt_layout(int sq, int n_out);
+
+// Backprojection tile shapes ("variants"): tx x ty voxels, vpt voxels per
+// thread, ca angles per staged chunk, win bins per staged window.
+constexpr int kBpVariants = 4;
+struct BpShape {
+    int tx, ty, vpt, ca, win;
+};
+BpShape bp_shape(int variant);
+// The shape used without tuning: a function of the job's size only.
+int bp_default_variant(int n_out, int nz, int sms);
 
 // FilterDesign (FilterDesign.cpp:13-111) in double precision: fft_size/2+1 values.
 std::vector<double> filter_response(int L, int type);
@@ -166,19 +176,19 @@ struct FiltBatch {
     FiltJob job[kMaxJobs];
 };
 BpJob make_bp_job(const float4* d_filt, int nz, int na, const FiltLayout& fl, int n_out, Trig trig,
-                  const float4* d_stats, int denorm, float* d_out);
+                  const float4* d_stats, int denorm, float* d_out, int variant);
 FiltJob make_filt_job(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
                       const float2* d_Hc, const float4* d_stats, int denorm, float scale,
                       float4* d_filt);
 // Backprojection of a batch (below 2^31 items) on a persistent grid: d_counter
 // (zeroed here on the stream) hands out the items. Filtering takes one CTA per
 // item.
-cudaError_t launch_backproject_batch(const BpBatch& b, unsigned* d_counter, unsigned* d_err,
+cudaError_t launch_backproject_batch(const BpBatch& b, int variant, unsigned* d_counter, unsigned* d_err,
                                      cudaStream_t st);
 cudaError_t launch_filter_batch(const FiltBatch& b, cudaStream_t st);
 cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltLayout& fl,
                                int n_out, Trig trig, const float4* d_stats, int denorm,
-                               float* d_out, unsigned* d_err, cudaStream_t st);
+                               float* d_out, unsigned* d_err, cudaStream_t st, int variant = 0);
 cudaError_t launch_point_count(const float* d_vol, long long total, float thr,
                                unsigned* d_block_counts, int blocks, cudaStream_t st);
 cudaError_t launch_point_write(const float* d_vol, int nx, int ny, long long total, float thr,
@@ -212,6 +222,12 @@ struct ctb_ctx {
     // Toeplitz tables per (bins, filter).
     int filter_mode = 0;
     std::map<std::pair<int, int>, ctb::GemmTable> gemm_tables;
+    // Backprojection tile shape: forced (>= 0), or per size bucket from the
+    // autotuner, or bp_default_variant.
+    int sms = 0;
+    int bp_variant = -1;
+    bool autotune = false;
+    std::map<std::vector<int>, int> tuned;  // {n bucket, angle bucket, slice-group bucket} -> variant
     // Angle tables: uniform angle sets per count; the last explicit list.
     std::map<int, ctb::DevBuf> trig_uniform;
     std::vector<float> user_angles;

@@ -165,6 +165,7 @@ struct ctb_server {
     ctb_arena arena;
     cudaStream_t compute = nullptr;
     cudaStream_t table_stream = nullptr;
+    int sms = 0;
     unsigned* d_err = nullptr;  // [0] error word of bounded waits, [1] backprojection item counter
     unsigned* h_err = nullptr;  // pinned, one word per batch slot
     std::vector<Stager> up_st, down_st;
@@ -347,23 +348,31 @@ ctb_status launch_batch(ctb_server* s, const std::vector<SReq*>& reqs, int slot)
         }
         if (launch_filter_batch(f, s->compute) != cudaSuccess) return CTB_ERR_CUDA;
     }
-    // one persistent backprojection launch, most angles first
+    // one persistent backprojection launch per tile shape (the default shape of
+    // each request, a function of its size), most angles first
+    std::vector<int> var(n);
+    for (int k = 0; k < n; ++k) var[k] = bp_default_variant(reqs[k]->r.output_size, reqs[k]->r.depth, s->sms);
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int b) { return reqs[a]->r.num_angles > reqs[b]->r.num_angles; });
-    BpBatch bp;
-    for (int k = 0; k < n; ++k) {
-        const SReq* q = reqs[order[k]];
-        Trig trig;
-        trig.cs = static_cast<const double2*>(q->d_trig);
-        trig.csf = reinterpret_cast<const float2*>(static_cast<const double2*>(q->d_trig) + q->r.num_angles);
-        BpJob J = make_bp_job(q->d_filt, q->r.depth, q->r.num_angles, q->fl, q->r.output_size, trig, nullptr,
-                              CTB_DENORM_NONE, q->d_out);
-        J.first = bp.total;
-        bp.total += static_cast<long long>(J.tiles) * ((J.nz + 3) / 4);
-        bp.job[bp.njobs++] = J;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return var[a] != var[b] ? var[a] < var[b] : reqs[a]->r.num_angles > reqs[b]->r.num_angles;
+    });
+    for (int k = 0; k < n;) {
+        BpBatch bp;
+        const int v = var[order[k]];
+        while (k < n && bp.njobs < kMaxJobs && var[order[k]] == v) {
+            const SReq* q = reqs[order[k]];
+            Trig trig;
+            trig.cs = static_cast<const double2*>(q->d_trig);
+            trig.csf = reinterpret_cast<const float2*>(static_cast<const double2*>(q->d_trig) + q->r.num_angles);
+            BpJob J = make_bp_job(q->d_filt, q->r.depth, q->r.num_angles, q->fl, q->r.output_size, trig, nullptr,
+                                  CTB_DENORM_NONE, q->d_out, v);
+            J.first = bp.total;
+            bp.total += static_cast<long long>(J.tiles) * ((J.nz + 3) / 4);
+            bp.job[bp.njobs++] = J;
+            ++k;
+        }
+        if (launch_backproject_batch(bp, v, s->d_err + 1, s->d_err, s->compute) != cudaSuccess) return CTB_ERR_CUDA;
     }
-    if (launch_backproject_batch(bp, s->d_err + 1, s->d_err, s->compute) != cudaSuccess) return CTB_ERR_CUDA;
     if (cudaMemcpyAsync(s->h_err + slot, s->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s->compute) !=
             cudaSuccess ||
         cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), s->compute) != cudaSuccess)
@@ -670,6 +679,7 @@ ctb_status ctb_server_create(const ctb_server_config* config, ctb_server** out) 
     }
     auto* s = new ctb_server();
     s->cfg = cfg;
+    s->sms = prop.multiProcessorCount;
     bool ok = cudaStreamCreateWithFlags(&s->compute, cudaStreamNonBlocking) == cudaSuccess &&
               cudaStreamCreateWithFlags(&s->table_stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaMalloc(&s->d_err, 2 * sizeof(unsigned)) == cudaSuccess &&
