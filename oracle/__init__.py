@@ -83,6 +83,9 @@ def _declare_oracle(L):
     L.orc_generator3d.argtypes = [i, i, i, f, i, ctypes.c_uint, _F32P, _F32P]
     L.orc_point_cloud.argtypes = [_F32P, i, i, i, f, p, ctypes.c_longlong,
                                   ctypes.POINTER(ctypes.c_longlong)]
+    L.orc_cc_sinogram_f64.argtypes = [_F32P, i, i, i, i, ctypes.c_double, _F32P, _F64P, _F32P]
+    L.orc_cc_reconstruct_slice_f64.argtypes = [_F64P, i, i, _F32P, i, i, f, f, _F64P]
+    L.orc_cc_reconstruct_volume_f64.argtypes = [_F32P, i, i, i, i, _F64P]
 
 
 def _ok(rc: int, what: str):
@@ -244,6 +247,41 @@ def point_cloud(vol: np.ndarray, thr: float) -> np.ndarray:
 
 
 # ------------------------------------------------------- error measures
+# ------------------------------------------- the CUDA backend's conventions
+def cc_sinogram_f64(slice2d: np.ndarray, na: int, nd: int, det_center=None, angles_deg=None):
+    """CUDABackend::computeSinogram restated in FP64 (ray march, bilinear,
+    every pixel normalised; detector centre (nd - 1) / 2 unless given).
+    Returns (sino[na][nd] f64, angles, minmax)."""
+    s = np.ascontiguousarray(slice2d, np.float32)
+    h, w = s.shape
+    ang = uniform_angles_deg(na) if angles_deg is None else np.ascontiguousarray(angles_deg, np.float32)
+    out = np.zeros((na, nd), np.float64)
+    mm = np.zeros(2, np.float32)
+    dc = 0.5 * (nd - 1) if det_center is None else float(det_center)
+    _ok(lib().orc_cc_sinogram_f64(s, w, h, na, nd, dc, ang, out, mm), "cc_sinogram_f64")
+    return out, ang, mm
+
+
+def cc_reconstruct_slice_f64(sino: np.ndarray, angles_deg, n_out: int, kind: int, min_hu=0.0, max_hu=0.0):
+    """CUDABackend::reconstructSlice restated in FP64 (Nyquist kept, (N-1)/2 and
+    (sq-1)/2 centres, per-tap bounds, denormalised when max_hu > min_hu)."""
+    s = np.ascontiguousarray(sino, np.float64)
+    na, nd = s.shape
+    out = np.zeros((n_out, n_out), np.float64)
+    _ok(lib().orc_cc_reconstruct_slice_f64(s, na, nd, np.ascontiguousarray(angles_deg, np.float32), n_out, kind,
+                                          float(min_hu), float(max_hu), out), "cc_reconstruct_slice_f64")
+    return out
+
+
+def cc_reconstruct_volume_f64(vol: np.ndarray, na: int, kind: int) -> np.ndarray:
+    """CUDABackend::reconstructVolume restated in FP64 (nd = n, detector centre floor(n / 2))."""
+    v = np.ascontiguousarray(vol, np.float32)
+    depth, n, _ = v.shape
+    out = np.zeros(v.shape, np.float64)
+    _ok(lib().orc_cc_reconstruct_volume_f64(v, n, depth, na, kind, out), "cc_reconstruct_volume_f64")
+    return out
+
+
 def rel_l2(a, b) -> float:
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)

@@ -224,6 +224,29 @@ void irfft_f64(const std::vector<cd>& X, std::vector<double>& x) {
     }
 }
 
+// Inverse real FFT that reads the Nyquist bin (the cuFFT C2R convention the
+// reference's CUDA backend uses, CUDABackend.cu:636), normalised like
+// irfft_f64.
+void irfft_full_f64(const std::vector<cd>& X, std::vector<double>& x) {
+    const size_t h = X.size() - 1;
+    std::vector<cd> z(h);
+    for (size_t k = 0; k < h; ++k) {
+        const cd xk = X[k];
+        const cd xm = std::conj(X[h - k]);
+        const cd ev = (xk + xm);
+        const cd od = (xk - xm) * cd(0, 1.0);
+        const double ang = kPiD * static_cast<double>(k) / static_cast<double>(h);
+        const cd w(std::cos(ang), std::sin(ang));
+        z[k] = ev + w * od;
+    }
+    fft_core_f64(z, true);
+    x.resize(2 * h);
+    for (size_t k = 0; k < h; ++k) {
+        x[2 * k] = z[k].real() * 0.5;
+        x[2 * k + 1] = z[k].imag() * 0.5;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Filter design — FilterDesign.cpp:13-111. Filter ids follow
 // ReconstructionParams::FilterType (CTTypes.h:151): Ramp, SheppLogan, Hamming,
@@ -736,6 +759,129 @@ int orc_point_cloud(const float* vol, int nx, int ny, int nz, float thr, float* 
                 }
             }
     *count = c;
+    return 0;
+}
+
+
+// ---------------------------------------------------------------------------
+// The reference's CUDA backend conventions (CUDABackend.cu), in double
+// precision: the FP64 restatement the CUDA-convention mode is checked against,
+// pinned by tests/golden/cuda_conv.npz (written by the reference itself).
+
+// CUDABackend::computeSinogram / radonForwardGatherKernel (CUDABackend.cu:
+// 108-153, 524-590): every pixel normalised (v - min) / span (span < 1e-6 -> 1),
+// rays through (cx + u cos, cy - u sin) with direction (sin, cos), u = bin -
+// det_center, samples t = -half + i for i < floor(2 half) + 1 (half =
+// sqrt(w^2 + h^2) / 2 in float), bilinear interpolation with zero outside.
+int orc_cc_sinogram_f64(const float* slice, int w, int h, int na, int nd, double det_center,
+                        const float* angles_deg, double* sino, float* minmax) {
+    if (!slice || w <= 0 || h <= 0 || na <= 0 || nd <= 0 || !angles_deg || !sino) return 1;
+    const size_t np = static_cast<size_t>(w) * h;
+    float lo = slice[0], hi = slice[0];
+    for (size_t i = 1; i < np; ++i) {
+        lo = std::min(lo, slice[i]);
+        hi = std::max(hi, slice[i]);
+    }
+    if (minmax) { minmax[0] = lo; minmax[1] = hi; }
+    float span = hi - lo;
+    if (span < 1e-6f) span = 1.0f;
+    std::vector<double> v(np);
+    for (size_t i = 0; i < np; ++i) v[i] = (static_cast<double>(slice[i]) - lo) / span;
+    const double cx = 0.5 * (w - 1), cy = 0.5 * (h - 1);
+    const float half_f = 0.5f * std::sqrt(static_cast<float>(w * w + h * h));
+    const int ns = static_cast<int>(2.0f * half_f) + 1;
+    auto at = [&](int x, int y) -> double {
+        return (x >= 0 && x < w && y >= 0 && y < h) ? v[static_cast<size_t>(y) * w + x] : 0.0;
+    };
+    for (int a = 0; a < na; ++a) {
+        const double th = static_cast<double>(angles_deg[a]) * kPiD / 180.0;
+        const double c = std::cos(th), sn = std::sin(th);
+        for (int b = 0; b < nd; ++b) {
+            const double u = b - det_center;
+            const double bx = cx + u * c, by = cy - u * sn;
+            double sum = 0.0;
+            for (int i = 0; i < ns; ++i) {
+                const double t = -static_cast<double>(half_f) + i;
+                const double x = bx + t * sn, y = by + t * c;
+                const int x0 = static_cast<int>(std::floor(x)), y0 = static_cast<int>(std::floor(y));
+                const double fx = x - x0, fy = y - y0;
+                sum += (1 - fx) * (1 - fy) * at(x0, y0) + fx * (1 - fy) * at(x0 + 1, y0) +
+                       (1 - fx) * fy * at(x0, y0 + 1) + fx * fy * at(x0 + 1, y0 + 1);
+            }
+            sino[static_cast<size_t>(a) * nd + b] = sum;
+        }
+    }
+    return 0;
+}
+
+// CUDABackend::reconstructSlice (CUDABackend.cu:592-690): rows padded to L at
+// pad_before, multiplied by H[k] for k = 0..L/2 (Nyquist kept), inverse / L,
+// first sq samples; backprojection with radius (n-1)/2, detector centre
+// (sq-1)/2, each tap read only when inside [0, sq), lerp v0 + (v1 - v0) frac,
+// x pi / (2 na); denormalised (x span + min) when max - min > 0.
+int orc_cc_reconstruct_slice_f64(const double* sino, int na, int nd, const float* angles_deg, int n_out,
+                                 int filter, float min_hu, float max_hu, double* out) {
+    if (!sino || na <= 0 || nd <= 0 || n_out <= 0 || !out || !angles_deg) return 1;
+    const PadGeom g = pad_geom(static_cast<size_t>(nd));
+    const std::vector<double> H = filter_f64(g.L, filter);
+    const size_t ns = g.L / 2 + 1;
+    std::vector<double> filt(static_cast<size_t>(na) * g.sq), padded(g.L), q;
+    std::vector<cd> spec;
+    for (int a = 0; a < na; ++a) {
+        std::fill(padded.begin(), padded.end(), 0.0);
+        for (int i = 0; i < nd; ++i) padded[i + g.pad] = sino[static_cast<size_t>(a) * nd + i];
+        rfft_f64(padded, spec);
+        for (size_t k = 0; k < ns; ++k) spec[k] *= H[k];
+        irfft_full_f64(spec, q);  // normalised inverse (the C2R result x 1 / L)
+        std::copy(q.begin(), q.begin() + g.sq, filt.begin() + static_cast<size_t>(a) * g.sq);
+    }
+    std::vector<double> ct(na), st(na);
+    for (int a = 0; a < na; ++a) {
+        const double th = static_cast<double>(angles_deg[a]) * kPiD / 180.0;
+        ct[a] = std::cos(th);
+        st[a] = std::sin(th);
+    }
+    const double radius = 0.5 * (n_out - 1), dc = 0.5 * (static_cast<double>(g.sq) - 1.0);
+    const double scale = kPiD / (2.0 * na);
+    const int sq = static_cast<int>(g.sq);
+    const double span = static_cast<double>(max_hu) - static_cast<double>(min_hu);
+    for (int y = 0; y < n_out; ++y) {
+        const double yy = y - radius;
+        for (int x = 0; x < n_out; ++x) {
+            const double xx = x - radius;
+            double r = 0.0;
+            if (!(xx * xx + yy * yy > radius * radius)) {
+                for (int a = 0; a < na; ++a) {
+                    const double u = xx * ct[a] - yy * st[a] + dc;
+                    const int i0 = static_cast<int>(std::floor(u));
+                    const double* f = filt.data() + static_cast<size_t>(a) * sq;
+                    const double v0 = (i0 >= 0 && i0 < sq) ? f[i0] : 0.0;
+                    const double v1 = (i0 + 1 >= 0 && i0 + 1 < sq) ? f[i0 + 1] : 0.0;
+                    r += v0 + (v1 - v0) * (u - i0);
+                }
+                r *= scale;
+            }
+            out[static_cast<size_t>(y) * n_out + x] = (max_hu - min_hu > 0.0f) ? r * span + min_hu : r;
+        }
+    }
+    return 0;
+}
+
+// CUDABackend::reconstructVolume (CUDABackend.cu:692-...): per slice the
+// forward projection onto nd = n bins with detector centre floor(n / 2), then
+// reconstructSlice with the slice's own min/max.
+int orc_cc_reconstruct_volume_f64(const float* vol, int n, int depth, int na, int filter, double* out) {
+    if (!vol || n <= 0 || depth <= 0 || na <= 0 || !out) return 1;
+    std::vector<float> ang(na);
+    const float step = 180.0f / static_cast<float>(na);
+    for (int a = 0; a < na; ++a) ang[a] = static_cast<float>(a) * step;
+    std::vector<double> sino(static_cast<size_t>(na) * n);
+    for (int z = 0; z < depth; ++z) {
+        float mm[2];
+        const size_t off = static_cast<size_t>(z) * n * n;
+        orc_cc_sinogram_f64(vol + off, n, n, na, n, static_cast<double>(n / 2), ang.data(), sino.data(), mm);
+        orc_cc_reconstruct_slice_f64(sino.data(), na, n, ang.data(), n, filter, mm[0], mm[1], out + off);
+    }
     return 0;
 }
 

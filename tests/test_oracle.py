@@ -3,6 +3,8 @@
 The float restatement must reproduce SerialBackend bit for bit on every golden
 case; the FP64 rerun must sit within the float path's known error.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -109,3 +111,34 @@ def test_openmp_fbp_matches_serial_fbp_on_same_sinogram(golden):
     ser = R.reconstruct_slice(R.SERIAL, sino, ang, n, kind, mm[0], mm[1])
     omp = R.reconstruct_slice(R.OPENMP, sino, ang, n, kind, 0.0, 1.0)  # span 1, min 0: identity
     assert O.rel_l2(omp, ser) < 1e-6
+
+
+# ------------------------------------------- the CUDA backend's conventions
+CUDA_CASES = ["ramp64", "shepp96", "hann128_even", "hamming80", "cosine48", "bartlett72"]
+
+
+@pytest.fixture(scope="module")
+def cuda_golden():
+    return np.load(os.path.join(os.path.dirname(__file__), "golden", "cuda_conv.npz"))
+
+
+@pytest.mark.parametrize("case", CUDA_CASES)
+def test_cuda_convention_oracle_pinned(cuda_golden, case):
+    """The FP64 restatement of CUDABackend against outputs of CUDABackend itself
+    (float arithmetic and cuFFT on the GPU): sinograms to 2e-6, reconstructions
+    to 1e-5 rel-L2."""
+    g = cuda_golden
+    n, na, nd, kind = (int(v) for v in g[f"{case}_meta"])
+    sino, ang, mm = O.cc_sinogram_f64(g[f"{case}_slice"], na, nd)
+    np.testing.assert_array_equal(mm, g[f"{case}_minmax"])
+    assert O.rel_l2(sino, g[f"{case}_sino"]) <= 2e-6
+    rec = O.cc_reconstruct_slice_f64(g[f"{case}_sino"], ang, n, kind, *g[f"{case}_minmax"])
+    assert O.rel_l2(rec, g[f"{case}_recon"]) <= 1e-5
+    assert O.max_abs_rel(rec, g[f"{case}_recon"]) <= 1e-5
+
+
+def test_cuda_convention_volume_pinned(cuda_golden):
+    g = cuda_golden
+    n, depth, na, kind = (int(v) for v in g["volume_meta"])
+    out = O.cc_reconstruct_volume_f64(g["volume_in"], na, kind)
+    assert O.rel_l2(out, g["volume_out"]) <= 1e-5
