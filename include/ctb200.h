@@ -65,7 +65,8 @@ typedef enum ctb_filter {
 typedef enum ctb_denorm {
     CTB_DENORM_NONE = 0,
     CTB_DENORM_SERIAL = 1,
-    CTB_DENORM_OPENMP = 2
+    CTB_DENORM_OPENMP = 2,
+    CTB_DENORM_CUDA = 3   /* out * span + min when span > 0, else out (CUDABackend.cu:676-681) */
 } ctb_denorm;
 
 /* ---------------------------------------------------------------- lifecycle */
@@ -135,6 +136,21 @@ ctb_status ctb_set_autotune(ctb_ctx* ctx, int enable);
 ctb_status ctb_autotune_table(ctb_ctx* ctx, int* entries, int capacity, int* count);
 ctb_status ctb_autotune_load(ctb_ctx* ctx, const int* entries, int count);
 
+/* Conventions of a context's host- and device-buffer entry points (batches
+ * and the serving loop always use SerialBackend's):
+ *   SERIAL  SerialBackend's (the default; the oracle): pixel splat forward
+ *           projector with zero pixels skipped, dropped Nyquist bin,
+ *           floor(n/2) / floor(sq/2) centres, both taps required;
+ *   CUDA    the reference's CUDA backend (CUDABackend.cu): every pixel
+ *           normalised, ray-march bilinear forward projector with detector
+ *           centre (nd-1)/2 for slices and floor(nd/2) for volumes
+ *           (:108-153, :534, :759), cuFFT-style filter keeping the Nyquist bin
+ *           (:603-652), backprojection with (n-1)/2 and (sq-1)/2 centres and
+ *           per-tap bounds (:184-236, :672), denormalisation only when
+ *           max > min (:676-681). */
+enum { CTB_CONVENTION_SERIAL = 0, CTB_CONVENTION_CUDA = 1 };
+ctb_status ctb_set_convention(ctb_ctx* ctx, int convention);
+
 /* Measured shared-memory load bandwidth of this GPU in GB/s: a conflict-free
  * 16-byte-per-lane load loop over all SMs, timed with CUDA events. The
  * backprojector's roofline denominator. */
@@ -164,6 +180,13 @@ ctb_status ctb_compute_sinogram(ctb_ctx* ctx, const float* slice, int width, int
 ctb_status ctb_reconstruct_slice(ctb_ctx* ctx, const float* sino, int num_angles,
                                  int detector_bins, const float* angles_deg, int output_size,
                                  int filter, float* out);
+/* reconstructSlice with the Sinogram's original_min_hu / original_max_hu: the
+ * CUDA convention denormalises with them when max > min (CUDABackend.cu:
+ * 676-681); the Serial convention ignores them (normalised units, as
+ * SerialBackend::reconstructSlice). ctb_reconstruct_slice = min = max = 0. */
+ctb_status ctb_reconstruct_slice_hu(ctb_ctx* ctx, const float* sino, int num_angles, int detector_bins,
+                                    const float* angles_deg, int output_size, int filter, float min_hu,
+                                    float max_hu, float* out);
 
 /* IReconstructionBackend::reconstructVolume (SerialBackend.cpp:261-318):
  * per slice, forward projection onto detector_bins bins (the reference passes

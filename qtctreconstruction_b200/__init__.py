@@ -43,6 +43,7 @@ class Denorm(enum.IntEnum):
     NONE = 0     # normalised units (SerialBackend::reconstructSlice)
     SERIAL = 1   # x * (span <= 0 ? 1 : span) + min  (SerialBackend.cpp:297-304)
     OPENMP = 2   # x * span + min, min if span <= 0  (OpenMPBackend.cpp:37-59)
+    CUDA = 3     # x * span + min if span > 0, else x  (CUDABackend.cu:676-681)
 
 
 @dataclass
@@ -103,6 +104,8 @@ class ServerStats(ctypes.Structure):
 
 
 REQ_DEVICE = 1     # CTB_REQ_DEVICE
+CONVENTION_SERIAL = 0       # CTB_CONVENTION_SERIAL
+CONVENTION_CUDA = 1         # CTB_CONVENTION_CUDA
 FILTER_MODE_FFT = 0         # CTB_FILTER_MODE_FFT
 FILTER_MODE_TC_BF16X3 = 1   # CTB_FILTER_MODE_TC_BF16X3
 BATCH_GRAPH = 1    # CTB_BATCH_GRAPH
@@ -143,6 +146,8 @@ def _declare(L):
     L.ctb_filter_response.argtypes = [i, i, _F32P]
     L.ctb_compute_sinogram.argtypes = [p, p, i, i, i, i, p, p, p]
     L.ctb_reconstruct_slice.argtypes = [p, p, i, i, p, i, i, p]
+    L.ctb_reconstruct_slice_hu.argtypes = [p, p, i, i, p, i, i, f, f, p]
+    L.ctb_set_convention.argtypes = [p, i]
     L.ctb_reconstruct_volume.argtypes = [p, p, i, i, i, i, i, p]
     L.ctb_reconstruct_from_sinograms.argtypes = [p, p, i, i, i, p, i, i, p]
     L.ctb_forward_d.argtypes = [p, p, i, i, i, i, p, p, p]
@@ -349,15 +354,19 @@ class B200Backend:
 
     def reconstructSlice(self, sinogram: Sinogram, output_size: int,
                          params: ReconstructionParams) -> np.ndarray:
-        """SerialBackend::reconstructSlice (SerialBackend.cpp:142-255): normalised units."""
+        """IReconstructionBackend::reconstructSlice: SerialBackend's normalised units
+        (SerialBackend.cpp:142-255), or with the CUDA convention the CUDA backend's
+        denormalisation by the sinogram's original_min_hu/max_hu (CUDABackend.cu:676-681)."""
         d = _f32(sinogram.data)
         if d.ndim != 2 or d.size == 0 or output_size <= 0:
             return np.zeros((0, 0), np.float32)
         na, nd = d.shape
         ang = _f32(sinogram.angles_deg)
         out = np.zeros((output_size, output_size), np.float32)
-        self._check(self._lib.ctb_reconstruct_slice(self._h, _ptr(d), na, nd, _ptr(ang), output_size,
-                                                    int(params.filter), _ptr(out)), "reconstructSlice")
+        self._check(self._lib.ctb_reconstruct_slice_hu(self._h, _ptr(d), na, nd, _ptr(ang), output_size,
+                                                       int(params.filter), float(sinogram.original_min_hu),
+                                                       float(sinogram.original_max_hu), _ptr(out)),
+                    "reconstructSlice")
         return out
 
     def reconstructVolume(self, volume, params: ReconstructionParams,
@@ -473,6 +482,10 @@ class B200Backend:
         """reconstructVolume through the host-buffer C ABI call on raw (e.g. pinned) pointers."""
         self._check(self._lib.ctb_reconstruct_volume(self._h, ctypes.c_void_p(host_vol), n, depth, na, nd,
                                                      int(kind), ctypes.c_void_p(host_out)), "reconstructVolume")
+
+    def set_convention(self, convention: int):
+        """CONVENTION_SERIAL (default, SerialBackend) or CONVENTION_CUDA (the reference CUDA backend)."""
+        self._check(self._lib.ctb_set_convention(self._h, int(convention)), "set_convention")
 
     def set_filter_mode(self, mode: int):
         """FILTER_MODE_FFT (default) or FILTER_MODE_TC_BF16X3 (tensor-core Toeplitz product)."""
@@ -751,6 +764,6 @@ GENERATOR3D_TISSUE = np.array(
     [-20.0, 45.0, 3.0, 10.0, 0.0, 0.0, 0.0, 1.0,
      200.0, 1000.0, 2.0, 8.0, 1.0, 0.7, 0.9, 0.15], dtype=np.float32)
 
-__all__ = ["bp_shape_info", "load_sinogram_file", "save_sinogram_file", "FILTER_MODE_FFT", "FILTER_MODE_TC_BF16X3", "B200Backend", "Batch", "Server", "Arena", "ServerConfig", "Request", "ServerStats", "REQ_DEVICE", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
+__all__ = ["CONVENTION_SERIAL", "CONVENTION_CUDA", "bp_shape_info", "load_sinogram_file", "save_sinogram_file", "FILTER_MODE_FFT", "FILTER_MODE_TC_BF16X3", "B200Backend", "Batch", "Server", "Arena", "ServerConfig", "Request", "ServerStats", "REQ_DEVICE", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
            "library", "pad_geometry", "filter_response", "uniform_angles_deg", "odd_detector_count",
            "phantom_params", "GENERATOR3D_TISSUE", "LIB_PATH"]

@@ -79,7 +79,7 @@ ctb_status fill_trig(ctb_ctx* ctx, const float* angles_deg, int na, void* table)
 ctb_status trig_table(ctb_ctx* ctx, const float* angles_deg, int na, Trig* out);
 // Cached convolution spectrum per (bins, filter) and twiddles per Lc.
 ctb_status filter_tables(ctb_ctx* ctx, const PadGeom& g, int type, const float2** d_Hc,
-                         const float2** d_tw);
+                         const float2** d_tw, bool keep_nyquist = false);
 // Reads and clears the device error word (synchronises the context's stream).
 ctb_status check_error_word(ctb_ctx* ctx);
 // Autotuner bucket of a backprojection job: {ceil(n / 64), ceil(na / 180),

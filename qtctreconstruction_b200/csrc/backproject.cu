@@ -124,22 +124,28 @@ __device__ __forceinline__ bool bp_tile(BpSmem<C>& S, const BpJob& J, int zg, in
     const int t = threadIdx.x;
     const int lx = t % XS, ly = t / XS;
     const int n = J.n, nz = J.nz, na = J.na, sq = J.sq;
-    const int rad = n / 2;
-    const float radf = static_cast<float>(rad);
+    const double ctr = J.ctr;  // voxel-grid centre (the mask radius too)
+    const float radf = static_cast<float>(ctr);
 
     float add[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int z = 4 * zg + j;
-        add[j] = (J.stats && J.denorm != CTB_DENORM_NONE && z < nz) ? J.stats[z].x : 0.0f;
+        float a = 0.0f;
+        if (J.stats && J.denorm != CTB_DENORM_NONE && z < nz) {
+            const float4 st = J.stats[z];
+            // CUDABackend.cu:676-681 adds the minimum only when max > min
+            a = (J.denorm == CTB_DENORM_CUDA && !(st.y - st.x > 0.0f)) ? 0.0f : st.x;
+        }
+        add[j] = a;
     }
 
     // Tiles entirely outside the reconstruction circle hold only the offset.
     {
         const int xe = min(x0 + TX - 1, n - 1), ye = min(y0 + TY - 1, n - 1);
-        const long long dx = max(0, max(x0 - rad, rad - xe));
-        const long long dy = max(0, max(y0 - rad, rad - ye));
-        if (dx * dx + dy * dy > static_cast<long long>(rad) * rad) {
+        const double dx = fmax(0.0, fmax(x0 - ctr, ctr - xe));
+        const double dy = fmax(0.0, fmax(y0 - ctr, ctr - ye));
+        if (dx * dx + dy * dy > ctr * ctr) {
             const int y = y0 + ly;
 #pragma unroll
             for (int k = 0; k < VPT; ++k) {
@@ -155,9 +161,9 @@ __device__ __forceinline__ bool bp_tile(BpSmem<C>& S, const BpJob& J, int zg, in
         }
     }
 
-    const double dcd = static_cast<double>(sq / 2);
-    const float dcf = static_cast<float>(sq / 2);
-    const double ox = static_cast<double>(x0 - rad), oy = static_cast<double>(y0 - rad);
+    const double dcd = J.dc;
+    const float dcf = static_cast<float>(J.dc);
+    const double ox = static_cast<double>(x0) - ctr, oy = static_cast<double>(y0) - ctr;
     const float4* plane = J.filt + static_cast<long long>(zg) * na * J.pitch;
     const int nch = (na + CA - 1) / CA;
 
@@ -180,7 +186,9 @@ __device__ __forceinline__ bool bp_tile(BpSmem<C>& S, const BpJob& J, int zg, in
             r.cf = tf.x;
             r.sf = tf.y;
             // taps near bin 0 or bin sq-1: the reference's float u decides them
-            r.edge = (umin < 2.0 || umax > sq - 3.0) ? 1 : 0;
+            // (the CUDA backend's per-tap bounds need no rule: bins outside
+            // [0, sq) are zeros of the guard)
+            r.edge = (J.edge_rule && (umin < 2.0 || umax > sq - 3.0)) ? 1 : 0;
             r.pad = 0;
             S.rec[b][t] = r;
             bulk_load(&S.win[b][t][0], plane + static_cast<long long>(a) * J.pitch + J.guard + ws,
@@ -252,8 +260,8 @@ __device__ __forceinline__ bool bp_tile(BpSmem<C>& S, const BpJob& J, int zg, in
                     const float u = fmaf(static_cast<float>(k), c8, ub);
                     const float fl = floorf(u);
                     const int i = static_cast<int>(fl);
-                    const float xs = static_cast<float>(x0 + lx + XS * k - rad);
-                    const float ys = static_cast<float>(y0 + ly - rad);
+                    const float xs = static_cast<float>(x0 + lx + XS * k) - radf;
+                    const float ys = static_cast<float>(y0 + ly) - radf;
                     const float us = __fadd_rn(__fsub_rn(__fmul_rn(xs, r.cf), __fmul_rn(ys, r.sf)), dcf);
                     const int is = static_cast<int>(floorf(us));
                     const bool ok = (is >= 0) && (is + 1 < sq);
@@ -407,7 +415,7 @@ FiltLayout filt_layout(int sq, int n_out) {
 }
 
 BpJob make_bp_job(const float4* d_filt, int nz, int na, const FiltLayout& fl, int n_out, Trig trig,
-                  const float4* d_stats, int denorm, float* d_out, int variant) {
+                  const float4* d_stats, int denorm, float* d_out, int variant, int convention) {
     const BpShape sh = bp_shape(variant);
     BpJob J;
     J.filt = d_filt;
@@ -421,6 +429,15 @@ BpJob make_bp_job(const float4* d_filt, int nz, int na, const FiltLayout& fl, in
     J.pitch = fl.pitch;
     J.n = n_out;
     J.denorm = denorm;
+    if (convention == kConvCuda) {  // CUDABackend.cu:205-224, 672
+        J.ctr = 0.5 * (n_out - 1);
+        J.dc = 0.5 * (fl.sq - 1);
+        J.edge_rule = 0;
+    } else {  // SerialBackend.cpp:205-224
+        J.ctr = static_cast<double>(n_out / 2);
+        J.dc = static_cast<double>(fl.sq / 2);
+        J.edge_rule = 1;
+    }
     J.tiles_x = (n_out + sh.tx - 1) / sh.tx;
     J.tiles = J.tiles_x * ((n_out + sh.ty - 1) / sh.ty);
     J.first = 0;
@@ -441,10 +458,10 @@ cudaError_t launch_backproject_batch(const BpBatch& b, int variant, unsigned* d_
 
 cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltLayout& fl,
                                int n_out, Trig trig, const float4* d_stats, int denorm,
-                               float* d_out, unsigned* d_err, cudaStream_t st, int variant) {
+                               float* d_out, unsigned* d_err, cudaStream_t st, int variant, int convention) {
     BpBatch b;
     b.njobs = 1;
-    b.job[0] = make_bp_job(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out, variant);
+    b.job[0] = make_bp_job(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out, variant, convention);
     b.total = static_cast<long long>(b.job[0].tiles) * ((nz + 3) / 4);
     if (b.total > 0x7fffffffLL) return cudaErrorInvalidValue;
     switch (variant) {

@@ -103,12 +103,12 @@ ctb_status trig_table(ctb_ctx* ctx, const float* angles_deg, int na, Trig* out) 
 // Convolution spectrum (conv_response) per (fft size, filter, bins), and the
 // twiddle table exp(-2 pi i k / Lc) per convolution length.
 ctb_status filter_tables(ctb_ctx* ctx, const PadGeom& g, int type, const float2** d_Hc,
-                         const float2** d_tw) {
+                         const float2** d_tw, bool keep_nyquist) {
     const int Lc = g.Lc;
-    auto key = std::make_pair(g.bins, type);
+    auto key = std::make_pair(g.bins, type + (keep_nyquist ? 16 : 0));
     auto it = ctx->filters.find(key);
     if (it == ctx->filters.end()) {
-        const std::vector<double> Hd = conv_response(g, type);
+        const std::vector<double> Hd = conv_response(g, type, keep_nyquist);
         std::vector<float2> Hc(Lc);
         for (int k = 0; k < Lc; ++k)
             Hc[k] = make_float2(static_cast<float>(Hd[2 * k]), static_cast<float>(Hd[2 * k + 1]));
@@ -199,9 +199,12 @@ ctb_status forward_plan_dev(ctb_ctx* ctx, const float* angles_deg, int na, int w
     return CTB_OK;
 }
 
+// volume_path selects the CUDA backend's volume detector centre floor(nd/2)
+// (CUDABackend.cu:759) instead of its slice centre (nd-1)/2 (:534); the
+// Serial convention has floor(nd/2) everywhere.
 ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz, int na, int nd,
                          const float* angles_deg, float* d_sino, float4* d_stats,
-                         cudaEvent_t* ev = nullptr) {
+                         cudaEvent_t* ev = nullptr, bool volume_path = false) {
     const int nzg = (nz + 3) / 4;
     const size_t elems = static_cast<size_t>(nzg) * std::max(fwd_plane_elems(h, w), fwd_plane_elems(w, h));
     CTB_WS(ctx, d_img, float4, "img", elems);
@@ -217,6 +220,13 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     Trig trig;
     CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
     CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream));
+    if (ctx->convention == kConvCuda) {
+        CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, nullptr, ctx->stream, 0));
+        mark(ctx, ev, 1);
+        const float det_center = volume_path ? static_cast<float>(nd / 2) : 0.5f * static_cast<float>(nd - 1);
+        CTB_LAUNCH(ctx, launch_raymarch(d_img, w, h, nz, na, nd, det_center, trig.cs, d_sino, ctx->stream));
+        return CTB_OK;
+    }
     CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream));
     mark(ctx, ev, 1);
     const ctb_ctx::FwdPlanDev* plan = nullptr;
@@ -242,11 +252,11 @@ ctb_status tune_backprojection(ctb_ctx* ctx, const float4* d_filt, int nz, int n
     int best_v = *variant;
     for (int v = 0; v < kBpVariants; ++v) {
         cudaError_t e = launch_backproject(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out, ctx->d_err,
-                                           ctx->stream, v);  // warm-up
+                                           ctx->stream, v, ctx->convention);  // warm-up
         if (e == cudaSuccess) e = cudaEventRecord(e0, ctx->stream);
         for (int r = 0; r < 2 && e == cudaSuccess; ++r)
             e = launch_backproject(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out, ctx->d_err,
-                                   ctx->stream, v);
+                                   ctx->stream, v, ctx->convention);
         if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -281,17 +291,18 @@ ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins
     CTB_WS(ctx, d_filt, float4, "filt", static_cast<size_t>(nzg) * na * fl.pitch);
     const float2* d_Hc = nullptr;
     const float2* d_tw = nullptr;
-    CTB_TRY(filter_tables(ctx, g, filter, &d_Hc, &d_tw));
+    const bool nyq = ctx->convention == kConvCuda;
+    CTB_TRY(filter_tables(ctx, g, filter, &d_Hc, &d_tw, nyq));
     Trig trig;
     CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
     // SerialBackend.cpp:246: pi / (2 na) in float
     const float scale = 3.14159265358979323846f / (2.0f * static_cast<float>(na));
     if (ctx->filter_mode == CTB_FILTER_MODE_TC_BF16X3) {
-        const auto key = std::make_pair(bins, filter);
+        const auto key = std::make_pair(bins, filter + (nyq ? 16 : 0));
         auto it = ctx->gemm_tables.find(key);
         if (it == ctx->gemm_tables.end()) {
             GemmTable tab;
-            CTB_CUDA(ctx, make_gemm_table(g, filter, &tab));
+            CTB_CUDA(ctx, make_gemm_table(g, filter, nyq, &tab));
             it = ctx->gemm_tables.emplace(key, tab).first;
         }
         CTB_WS(ctx, d_split, unsigned char, "gemm_split", filter_gemm_split_bytes(nz, na, bins));
@@ -309,7 +320,7 @@ ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins
     if (ctx->autotune && ctx->bp_variant < 0 && !ctx->tuned.count(bp_bucket(n_out, nz, na)))
         CTB_TRY(tune_backprojection(ctx, d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out, &variant));
     CTB_LAUNCH(ctx, launch_backproject(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out,
-                                       ctx->d_err, ctx->stream, variant));
+                                       ctx->d_err, ctx->stream, variant, ctx->convention));
     return CTB_OK;
 }
 
@@ -486,6 +497,13 @@ ctb_status ctb_autotune_load(ctb_ctx* ctx, const int* entries, int count) {
     return CTB_OK;
 }
 
+ctb_status ctb_set_convention(ctb_ctx* ctx, int convention) {
+    if (!ctx || (convention != CTB_CONVENTION_SERIAL && convention != CTB_CONVENTION_CUDA)) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    ctx->convention = convention;
+    return CTB_OK;
+}
+
 ctb_status ctb_set_filter_mode(ctb_ctx* ctx, int mode) {
     if (!ctx || (mode != CTB_FILTER_MODE_FFT && mode != CTB_FILTER_MODE_TC_BF16X3)) return CTB_ERR_INVALID;
     Guard g(ctx);
@@ -569,7 +587,7 @@ ctb_status ctb_fbp_d(ctb_ctx* ctx, const float* d_sino, int depth, int num_angle
                      int denorm, float* d_out) {
     CTB_TRY(check_common(ctx));
     if (!d_sino || !d_out || depth <= 0 || num_angles <= 0 || bins <= 0 || output_size <= 0 ||
-        num_angles > kMaxAngles || denorm < 0 || denorm > 2)
+        num_angles > kMaxAngles || denorm < 0 || denorm > CTB_DENORM_CUDA)
         return fail(ctx, CTB_ERR_INVALID, "ctb_fbp_d: invalid arguments");
     if (d_stats && !aligned16(d_stats)) return fail(ctx, CTB_ERR_INVALID, "d_stats must be 16-byte aligned");
     Guard g(ctx);
@@ -595,11 +613,11 @@ ctb_status ctb_reconstruct_volume_d(ctb_ctx* ctx, const float* d_vol, int n, int
     CTB_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
     mark(ctx, pev, 0);
     CTB_TRY(forward_stage(ctx, d_vol, n, n, depth, num_angles, detector_bins, nullptr, d_sino, d_stats,
-                          pev));
+                          pev, true));
     CTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
     mark(ctx, pev, 2);
     CTB_TRY(fbp_stage(ctx, d_sino, depth, num_angles, detector_bins, nullptr, n, filter, d_stats,
-                      CTB_DENORM_SERIAL, d_out, pev));
+                      ctx->convention == kConvCuda ? CTB_DENORM_CUDA : CTB_DENORM_SERIAL, d_out, pev));
     CTB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
     mark(ctx, pev, 4);
     return CTB_OK;
@@ -641,6 +659,13 @@ ctb_status ctb_compute_sinogram(ctb_ctx* ctx, const float* slice, int width, int
 ctb_status ctb_reconstruct_slice(ctb_ctx* ctx, const float* sino, int num_angles,
                                  int detector_bins, const float* angles_deg, int output_size,
                                  int filter, float* out) {
+    return ctb_reconstruct_slice_hu(ctx, sino, num_angles, detector_bins, angles_deg, output_size, filter,
+                                    0.0f, 0.0f, out);
+}
+
+ctb_status ctb_reconstruct_slice_hu(ctb_ctx* ctx, const float* sino, int num_angles, int detector_bins,
+                                    const float* angles_deg, int output_size, int filter, float min_hu,
+                                    float max_hu, float* out) {
     CTB_TRY(check_common(ctx));
     if (!sino || !out || !angles_deg || num_angles <= 0 || detector_bins <= 0 ||
         output_size <= 0 || num_angles > kMaxAngles)
@@ -650,10 +675,18 @@ ctb_status ctb_reconstruct_slice(ctb_ctx* ctx, const float* sino, int num_angles
     const size_t no = static_cast<size_t>(output_size) * output_size;
     CTB_WS(ctx, d_sino, float, "h_sino", ns);
     CTB_WS(ctx, d_out, float, "h_out", no);
+    CTB_WS(ctx, d_stats, float4, "h_stats", 1);
     CTB_CUDA(ctx, cudaMemcpyAsync(d_sino, sino, ns * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    // the CUDA backend denormalises with the sinogram's HU range (CUDABackend.cu:676-681);
+    // SerialBackend::reconstructSlice returns normalised units
+    const bool hu = ctx->convention == kConvCuda && max_hu - min_hu > 0.0f;
+    if (hu) {
+        const float4 st = make_float4(min_hu, max_hu, max_hu - min_hu, max_hu - min_hu);
+        CTB_CUDA(ctx, cudaMemcpyAsync(d_stats, &st, sizeof st, cudaMemcpyHostToDevice, ctx->stream));
+    }
     CTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
     CTB_TRY(fbp_stage(ctx, d_sino, 1, num_angles, detector_bins, angles_deg, output_size, filter,
-                      nullptr, CTB_DENORM_NONE, d_out));
+                      hu ? d_stats : nullptr, hu ? CTB_DENORM_CUDA : CTB_DENORM_NONE, d_out));
     CTB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
     CTB_CUDA(ctx, cudaMemcpyAsync(out, d_out, no * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -689,7 +722,7 @@ ctb_status ctb_reconstruct_from_sinograms(ctb_ctx* ctx, const float* sinos, int 
                                           int filter, int denorm, float* out) {
     CTB_TRY(check_common(ctx));
     if (!sinos || !out || !angles_deg || depth <= 0 || num_angles <= 0 || bins <= 0 ||
-        denorm < 0 || denorm > 2)
+        denorm < 0 || denorm > CTB_DENORM_CUDA)
         return fail(ctx, CTB_ERR_INVALID, "ctb_reconstruct_from_sinograms: invalid arguments");
     Guard g(ctx);
     const size_t ns = static_cast<size_t>(depth) * num_angles * bins;

@@ -29,11 +29,11 @@ PadGeom pad_geometry(int bins);
 // <= Lc samples, so the same linear operator is a circular convolution of length
 // Lc with h restricted to those lags. Returns DFT_Lc of that kernel divided by Lc
 // (re, im interleaved), evaluated in double precision.
-std::vector<double> conv_response(const PadGeom& g, int type);
+std::vector<double> conv_response(const PadGeom& g, int type, bool keep_nyquist = false);
 // The same kernel in the lag domain: h(d) for d = -(pad + bins - 1) .. sq - 1 - pad
 // (index d + pad + bins - 1), double precision. Filtered bin i of a row x is
 // sum_j h(i - pad - j) x[j].
-std::vector<double> conv_kernel(const PadGeom& g, int type);
+std::vector<double> conv_kernel(const PadGeom& g, int type, bool keep_nyquist = false);
 
 // Layout of the filtered rows the backprojector reads: for each group of four
 // slices and each angle, `pitch` bins of float4 (one float per slice), with
@@ -84,7 +84,11 @@ cudaError_t launch_trig(const float* d_angles_deg, int na, double2* d_cs, cudaSt
 cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4* d_stats,
                                cudaStream_t st);
 cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
-                             float4* d_img, float4* d_imgT, cudaStream_t st);
+                             float4* d_img, float4* d_imgT, cudaStream_t st, int skip_zero = 1);
+// The reference CUDA backend's ray-march forward projector over the
+// normalised image planes (img only).
+cudaError_t launch_raymarch(const float4* d_img, int w, int h, int nz, int na, int nd, float det_center,
+                            const double2* d_cs, float* d_sino, cudaStream_t st);
 // Forward projector work plan: angles grouped (up to kFwdGroup per CTA) by
 // walked axis so that one staged row segment of kFwdWidth pixels serves every
 // angle of the group. groups: {first index into order, count, axis (0 rows,
@@ -123,7 +127,7 @@ struct GemmTable {
     alignas(64) unsigned char map_hi[128];
     alignas(64) unsigned char map_lo[128];
 };
-cudaError_t make_gemm_table(const PadGeom& g, int type, GemmTable* out);
+cudaError_t make_gemm_table(const PadGeom& g, int type, bool keep_nyquist, GemmTable* out);
 int gemm_kpad(int bins);
 // Device bytes of the BF16 row split the tensor-core filter needs.
 size_t filter_gemm_split_bytes(int nz, int na, int bins);
@@ -148,7 +152,10 @@ struct BpJob {
     float* out;           // [nz][n][n]
     const float4* stats;  // per-slice {min, max, ...} or null
     Trig trig;
+    double ctr;           // voxel-grid centre: floor(n/2) (SerialBackend) or (n-1)/2 (CUDA backend)
+    double dc;            // detector centre: floor(sq/2) or (sq-1)/2
     int nz, na, sq, guard, pitch, n, denorm;
+    int edge_rule;        // 1: SerialBackend's tap rule (both taps in range); 0: per-tap bounds
     int tiles_x, tiles;   // tiles per row / per slice group
     long long first;      // index of the job's first item in the batch
 };
@@ -175,8 +182,11 @@ struct FiltBatch {
     const float2* tw = nullptr;  // exp(-2 pi i k / Lc)
     FiltJob job[kMaxJobs];
 };
+// Conventions of a reconstruction: SerialBackend's (the default, the oracle)
+// or the reference CUDA backend's (CUDABackend.cu).
+enum Convention { kConvSerial = 0, kConvCuda = 1 };
 BpJob make_bp_job(const float4* d_filt, int nz, int na, const FiltLayout& fl, int n_out, Trig trig,
-                  const float4* d_stats, int denorm, float* d_out, int variant);
+                  const float4* d_stats, int denorm, float* d_out, int variant, int convention = kConvSerial);
 FiltJob make_filt_job(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
                       const float2* d_Hc, const float4* d_stats, int denorm, float scale,
                       float4* d_filt);
@@ -188,7 +198,8 @@ cudaError_t launch_backproject_batch(const BpBatch& b, int variant, unsigned* d_
 cudaError_t launch_filter_batch(const FiltBatch& b, cudaStream_t st);
 cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltLayout& fl,
                                int n_out, Trig trig, const float4* d_stats, int denorm,
-                               float* d_out, unsigned* d_err, cudaStream_t st, int variant = 0);
+                               float* d_out, unsigned* d_err, cudaStream_t st, int variant = 0,
+                               int convention = kConvSerial);
 cudaError_t launch_point_count(const float* d_vol, long long total, float thr,
                                unsigned* d_block_counts, int blocks, cudaStream_t st);
 cudaError_t launch_point_write(const float* d_vol, int nx, int ny, long long total, float thr,
@@ -221,6 +232,7 @@ struct ctb_ctx {
     // Filter implementation (ctb_set_filter_mode) and the tensor-core path's
     // Toeplitz tables per (bins, filter).
     int filter_mode = 0;
+    int convention = 0;  // CTB_CONVENTION_SERIAL / CTB_CONVENTION_CUDA
     std::map<std::pair<int, int>, ctb::GemmTable> gemm_tables;
     // Backprojection tile shape: forced (>= 0), or per size bucket from the
     // autotuner, or bp_default_variant.

@@ -292,6 +292,7 @@ __device__ __forceinline__ float slice_scale(const float4* stats, int z, int nz,
     const float4 st = stats[z];
     const float span = st.y - st.x;
     if (denorm == CTB_DENORM_SERIAL) return scale * (span <= 0.0f ? 1.0f : span);
+    if (denorm == CTB_DENORM_CUDA) return span > 0.0f ? scale * span : scale;
     return span > 0.0f ? scale * span : 0.0f;  // OpenMP: span <= 0 -> min everywhere
 }
 

@@ -136,6 +136,7 @@ __device__ __forceinline__ float row_scale(const float4* stats, int z, int nz, i
     const float4 st = stats[z];
     const float span = st.y - st.x;
     if (denorm == CTB_DENORM_SERIAL) return scale * (span <= 0.0f ? 1.0f : span);
+    if (denorm == CTB_DENORM_CUDA) return span > 0.0f ? scale * span : scale;
     return span > 0.0f ? scale * span : 0.0f;
 }
 
@@ -348,13 +349,13 @@ size_t filter_gemm_split_bytes(int nz, int na, int bins) {
     return static_cast<size_t>(rows) * gemm_kpad(bins) * 2 * sizeof(__nv_bfloat16);
 }
 
-cudaError_t make_gemm_table(const PadGeom& g, int type, GemmTable* out) {
+cudaError_t make_gemm_table(const PadGeom& g, int type, bool keep_nyquist, GemmTable* out) {
     static_assert(sizeof(CUtensorMap) == sizeof(out->map_hi), "tensor map size");
     const int ntiles = (g.sq + BNMAX - 1) / BNMAX;
     const int bn = 16 * ((g.sq + 16 * ntiles - 1) / (16 * ntiles));
     const int nrows = ntiles * bn;
     const int kpad = gemm_kpad(g.bins);
-    const std::vector<double> h = conv_kernel(g, type);
+    const std::vector<double> h = conv_kernel(g, type, keep_nyquist);
     const int dmin = -(g.pad + g.bins - 1);
     std::vector<unsigned short> th(static_cast<size_t>(nrows) * kpad, 0), tl(th.size(), 0);
     for (int i = 0; i < g.sq; ++i)

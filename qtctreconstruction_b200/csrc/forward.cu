@@ -67,13 +67,16 @@ __global__ void __launch_bounds__(1024) k_slice_stats(const float* __restrict__ 
 // --------------------------------------------------------------- normalise
 // img[zg][y][x] = (v(4zg), v(4zg+1), v(4zg+2), v(4zg+3)) and imgT[zg][x][y], with
 // v = (raw - min) * (1 / span_fwd) for raw != 0 and v = 0 for raw == 0: the
-// reference skips background pixels (SerialBackend.cpp:104-106). Both copies
+// reference skips background pixels (SerialBackend.cpp:104-106). With
+// skip_zero = 0 every pixel is normalised, as the reference's CUDA backend does
+// (CUDABackend.cu:46-50); imgT may then be null (the ray march reads rows). Both copies
 // use the zero-bordered layout of the projector (kFwdGuard pixels left and
 // right of every row, kFwdRows rows below the last); only the interior is
 // written here, the borders are zeroed when the buffers are set up.
 __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol, int w, int h, int nz,
                                                    const float4* __restrict__ stats,
-                                                   float4* __restrict__ img, float4* __restrict__ imgT) {
+                                                   float4* __restrict__ img, float4* __restrict__ imgT,
+                                                   int skip_zero) {
     const long long pw = w + 2 * kFwdGuard, ph = h + 2 * kFwdGuard;  // row pitches
     const long long rw = h + kFwdRows, rh = w + kFwdRows;             // rows per plane
     __shared__ float4 tile[32][33];
@@ -99,7 +102,7 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
             for (int j = 0; j < 4; ++j) {
                 if (!live[j]) continue;
                 const float raw = __ldg(vol + (static_cast<long long>(4 * zg + j) * h + y) * w + x);
-                v[j] = (raw == 0.0f) ? 0.0f : __fmul_rn(__fsub_rn(raw, lo[j]), inv[j]);
+                v[j] = (skip_zero && raw == 0.0f) ? 0.0f : __fmul_rn(__fsub_rn(raw, lo[j]), inv[j]);
             }
         }
         const float4 q = make_float4(v[0], v[1], v[2], v[3]);
@@ -110,11 +113,93 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int x = x0 + ty + 8 * r, y = y0 + tx;
-        if (x < w && y < h) imgT[(zg * rh + x) * ph + y + kFwdGuard] = tile[tx][ty + 8 * r];
+        if (imgT && x < w && y < h) imgT[(zg * rh + x) * ph + y + kFwdGuard] = tile[tx][ty + 8 * r];
+    }
+}
+
+// ------------------------------------------------------------- ray march
+// The reference CUDA backend's forward projector (radonForwardGatherKernel,
+// CUDABackend.cu:108-153): the ray of bin b at angle a passes through
+// (cx + u cos, cy - u sin), u = b - det_center, with direction (sin, cos);
+// samples t = -half + i, i < floor(2 half) + 1 (half = sqrt(w^2 + h^2) / 2),
+// each the bilinear interpolation of the normalised image, zero outside. A
+// thread owns one (bin, angle) for four slices (one float4 image plane). Only
+// samples whose bilinear footprint can touch the image are visited (the
+// others add exact zeros in the reference): the parameter range is clipped to
+// -1 < x < w, -1 < y < h in double and widened by one sample each side. Pixel
+// columns read lie in [-2, w + 1] (inside the zero border); rows above the
+// image are skipped explicitly, rows below it are the zero rows of the plane.
+__global__ void __launch_bounds__(128) k_raymarch(const float4* __restrict__ img, int w, int h, int nz, int na,
+                                                  int nd, float det_center, const double2* __restrict__ cs,
+                                                  float* __restrict__ sino) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = blockIdx.y;
+    const int zg = blockIdx.z;
+    if (b >= nd) return;
+    const long long pitch = w + 2 * kFwdGuard;
+    const float4* plane = img + static_cast<long long>(zg) * (h + kFwdRows) * pitch + kFwdGuard;
+    const double2 tc = cs[a];
+    const float c = static_cast<float>(tc.x), s = static_cast<float>(tc.y);
+    const float cx = 0.5f * static_cast<float>(w - 1), cy = 0.5f * static_cast<float>(h - 1);
+    const float u = static_cast<float>(b) - det_center;
+    const float bx = cx + u * c, by = cy - u * s;
+    const float half = 0.5f * sqrtf(static_cast<float>(w * w + h * h));
+    const int ns = static_cast<int>(2.0f * half) + 1;
+    // parameter range with -1 < x(t) < w and -1 < y(t) < h
+    double tlo = -1e30, thi = 1e30;
+    const double sd = s, cd = c;
+    if (fabs(sd) > 1e-12) {
+        const double t0 = (-1.0 - bx) / sd, t1 = (w - static_cast<double>(bx)) / sd;
+        tlo = fmax(tlo, fmin(t0, t1));
+        thi = fmin(thi, fmax(t0, t1));
+    } else if (!(bx > -1.0f && bx < static_cast<float>(w))) {
+        thi = -2e30;
+    }
+    if (fabs(cd) > 1e-12) {
+        const double t0 = (-1.0 - by) / cd, t1 = (h - static_cast<double>(by)) / cd;
+        tlo = fmax(tlo, fmin(t0, t1));
+        thi = fmin(thi, fmax(t0, t1));
+    } else if (!(by > -1.0f && by < static_cast<float>(h))) {
+        thi = -2e30;
+    }
+    float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (thi >= tlo) {
+        const int i0 = max(0, static_cast<int>(floor(tlo + half)) - 1);
+        const int i1 = min(ns - 1, static_cast<int>(ceil(thi + half)) + 1);
+        for (int i = i0; i <= i1; ++i) {
+            const float t = static_cast<float>(i) - half;
+            const float x = bx + t * s, y = by + t * c;
+            const float xf = floorf(x), yf = floorf(y);
+            const int x0 = static_cast<int>(xf), y0 = static_cast<int>(yf);
+            const float fx = x - xf, fy = y - yf;
+            const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4* r0 = plane + static_cast<long long>(y0) * pitch + x0;
+            const float4 v00 = y0 >= 0 ? r0[0] : zero, v10 = y0 >= 0 ? r0[1] : zero;
+            const float4 v01 = y0 + 1 >= 0 ? r0[pitch] : zero, v11 = y0 + 1 >= 0 ? r0[pitch + 1] : zero;
+            const float w00 = (1.0f - fx) * (1.0f - fy), w10 = fx * (1.0f - fy);
+            const float w01 = (1.0f - fx) * fy, w11 = fx * fy;
+            sum.x += w00 * v00.x + w10 * v10.x + w01 * v01.x + w11 * v11.x;
+            sum.y += w00 * v00.y + w10 * v10.y + w01 * v01.y + w11 * v11.y;
+            sum.z += w00 * v00.z + w10 * v10.z + w01 * v01.z + w11 * v11.z;
+            sum.w += w00 * v00.w + w10 * v10.w + w01 * v01.w + w11 * v11.w;
+        }
+    }
+    const float v[4] = {sum.x, sum.y, sum.z, sum.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int z = 4 * zg + j;
+        if (z < nz) sino[(static_cast<long long>(z) * na + a) * nd + b] = v[j];
     }
 }
 
 }  // namespace
+
+cudaError_t launch_raymarch(const float4* d_img, int w, int h, int nz, int na, int nd, float det_center,
+                            const double2* d_cs, float* d_sino, cudaStream_t st) {
+    const dim3 grid((nd + 127) / 128, na, (nz + 3) / 4);
+    k_raymarch<<<grid, 128, 0, st>>>(d_img, w, h, nz, na, nd, det_center, d_cs, d_sino);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_trig(const float* d_angles_deg, int na, double2* d_cs, cudaStream_t st) {
     k_trig<<<(na + 127) / 128, 128, 0, st>>>(d_angles_deg, na, d_cs);
@@ -128,9 +213,9 @@ cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4
 }
 
 cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
-                             float4* d_img, float4* d_imgT, cudaStream_t st) {
+                             float4* d_img, float4* d_imgT, cudaStream_t st, int skip_zero) {
     const dim3 grid((w + 31) / 32, (h + 31) / 32, (nz + 3) / 4);
-    k_normalize<<<grid, 256, 0, st>>>(d_vol, w, h, nz, d_stats, d_img, d_imgT);
+    k_normalize<<<grid, 256, 0, st>>>(d_vol, w, h, nz, d_stats, d_img, d_imgT, skip_zero);
     return cudaGetLastError();
 }
 

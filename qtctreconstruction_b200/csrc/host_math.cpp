@@ -54,14 +54,16 @@ PadGeom pad_geometry(int bins) {
     return g;
 }
 
-std::vector<double> conv_kernel(const PadGeom& g, int type) {
+std::vector<double> conv_kernel(const PadGeom& g, int type, bool keep_nyquist) {
     const int L = g.L;
     const std::vector<double> H = filter_response(L, type);
     // h = IDFT_L(H~): H~ is real and even, so h = Re FFT_L(H~) / L (real, even)
     std::vector<std::complex<double>> t(L);
     for (int k = 0; k < L; ++k) t[k] = H[k <= L / 2 ? k : L - k];
     t[0] = 0.0;
-    t[L / 2] = 0.0;
+    // SerialBackend's inverse FFT never reads the Nyquist bin (FFT.cpp:96); the
+    // CUDA backend's cuFFT C2R does (CUDABackend.cu:636)
+    if (!keep_nyquist) t[L / 2] = 0.0;
     fft64(t);
     const int dmin = -(g.pad + g.bins - 1), dmax = g.sq - 1 - g.pad;
     std::vector<double> h(dmax - dmin + 1);
@@ -69,9 +71,9 @@ std::vector<double> conv_kernel(const PadGeom& g, int type) {
     return h;
 }
 
-std::vector<double> conv_response(const PadGeom& g, int type) {
+std::vector<double> conv_response(const PadGeom& g, int type, bool keep_nyquist) {
     const int Lc = g.Lc;
-    const std::vector<double> h = conv_kernel(g, type);
+    const std::vector<double> h = conv_kernel(g, type, keep_nyquist);
     std::vector<std::complex<double>> hc(Lc, 0.0);
     const int dmin = -(g.pad + g.bins - 1);
     for (size_t k = 0; k < h.size(); ++k) {
