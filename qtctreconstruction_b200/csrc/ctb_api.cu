@@ -244,7 +244,7 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
 // the output is that shape's.
 ctb_status tune_backprojection(ctb_ctx* ctx, const float4* d_filt, int nz, int na, const FiltLayout& fl,
                                int n_out, Trig trig, const float4* d_stats, int denorm, float* d_out,
-                               int* variant) {
+                               int* variant, int bucket_depth) {
     cudaEvent_t e0, e1;
     CTB_CUDA(ctx, cudaEventCreate(&e0));
     CTB_CUDA(ctx, cudaEventCreate(&e1));
@@ -274,14 +274,16 @@ ctb_status tune_backprojection(ctb_ctx* ctx, const float4* d_filt, int nz, int n
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    ctx->tuned[bp_bucket(n_out, nz, na)] = best_v;
+    ctx->tuned[bp_bucket(n_out, bucket_depth, na)] = best_v;
     *variant = best_v;
     return CTB_OK;
 }
 
+// shape_depth: the depth the backprojection tile shape is chosen for (a slab
+// of a volume uses the whole volume's, so slabs reproduce one pass bit for bit)
 ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins,
                      const float* angles_deg, int n_out, int filter, const float4* d_stats,
-                     int denorm, float* d_out, cudaEvent_t* ev = nullptr) {
+                     int denorm, float* d_out, cudaEvent_t* ev = nullptr, int shape_depth = 0) {
     const PadGeom g = pad_geometry(bins);
     if (g.Lc > kMaxFft)
         return fail(ctx, CTB_ERR_UNSUPPORTED, "convolution length %d (bins %d) exceeds %d", g.Lc, bins,
@@ -316,9 +318,10 @@ ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins
                                       ctx->stream));
     }
     mark(ctx, ev, 3);
-    int variant = bp_variant_for(ctx, n_out, nz, na);
-    if (ctx->autotune && ctx->bp_variant < 0 && !ctx->tuned.count(bp_bucket(n_out, nz, na)))
-        CTB_TRY(tune_backprojection(ctx, d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out, &variant));
+    const int zs = shape_depth > 0 ? shape_depth : nz;
+    int variant = bp_variant_for(ctx, n_out, zs, na);
+    if (ctx->autotune && ctx->bp_variant < 0 && !ctx->tuned.count(bp_bucket(n_out, zs, na)))
+        CTB_TRY(tune_backprojection(ctx, d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out, &variant, zs));
     CTB_LAUNCH(ctx, launch_backproject(d_filt, nz, na, fl, n_out, trig, d_stats, denorm, d_out,
                                        ctx->d_err, ctx->stream, variant, ctx->convention));
     return CTB_OK;
@@ -399,6 +402,9 @@ void ctb_destroy(ctb_ctx* ctx) {
         for (auto& e : ctx->ev)
             if (e) cudaEventDestroy(e);
         if (ctx->d_err) cudaFree(ctx->d_err);
+        for (auto& e : ctx->slab_ev) cudaEventDestroy(e);
+        if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
+        if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     }
     delete ctx;
@@ -699,21 +705,77 @@ ctb_status ctb_reconstruct_slice_hu(ctb_ctx* ctx, const float* sino, int num_ang
 ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int depth,
                                   int num_angles, int detector_bins, int filter, float* out) {
     CTB_TRY(check_common(ctx));
-    if (!vol || !out || n <= 0 || depth <= 0 || num_angles <= 0 || detector_bins <= 0)
+    if (!vol || !out || n <= 0 || depth <= 0 || num_angles <= 0 || detector_bins <= 0 ||
+        num_angles > kMaxAngles)
         return fail(ctx, CTB_ERR_INVALID, "ctb_reconstruct_volume: invalid arguments");
     Guard g(ctx);
-    const size_t nv = static_cast<size_t>(depth) * n * n;
-    CTB_WS(ctx, d_in, float, "h_in", nv);
-    CTB_WS(ctx, d_out, float, "h_out", nv);
-    CTB_CUDA(ctx, cudaMemcpyAsync(d_in, vol, nv * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-    CTB_TRY(ctb_reconstruct_volume_d(ctx, d_in, n, depth, num_angles, detector_bins, filter, d_out));
-    CTB_CUDA(ctx, cudaMemcpyAsync(out, d_out, nv * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    // Slabs of whole slice groups: the host->device copy of slab k + 1 and the
+    // device->host copy of slab k - 1 run on their own streams while slab k is
+    // reconstructed; slices are independent, so the result is the same as one
+    // pass over the volume. Two slab buffers each way.
+    constexpr int kSlabs = 8;
+    const int slab = depth <= 16 ? depth : 4 * ((depth + 4 * kSlabs - 1) / (4 * kSlabs));
+    const int nslab = (depth + slab - 1) / slab;
+    const size_t per = static_cast<size_t>(slab) * n * n;
+    CTB_WS(ctx, d_in, float, "h_in", 2 * per);
+    CTB_WS(ctx, d_out, float, "h_out", 2 * per);
+    CTB_WS(ctx, d_sino, float, "sino", static_cast<size_t>(slab) * num_angles * detector_bins);
+    CTB_WS(ctx, d_stats, float4, "stats", slab);
+    if (!ctx->copy_in) {
+        CTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
+        CTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
+    }
+    // events: per buffer {input landed, slab computed, output copied}; per slab {start, forward done, end}
+    const size_t need = 6 + 3 * static_cast<size_t>(nslab);
+    while (ctx->slab_ev.size() < need) {
+        cudaEvent_t e;
+        CTB_CUDA(ctx, cudaEventCreate(&e));
+        ctx->slab_ev.push_back(e);
+    }
+    cudaEvent_t* in_done = &ctx->slab_ev[0];
+    cudaEvent_t* computed = &ctx->slab_ev[2];
+    cudaEvent_t* out_done = &ctx->slab_ev[4];
+    cudaEvent_t* t = &ctx->slab_ev[6];
+    CTB_CUDA(ctx, cudaEventRecord(computed[0], ctx->stream));  // buffers start free
+    CTB_CUDA(ctx, cudaEventRecord(computed[1], ctx->stream));
+    CTB_CUDA(ctx, cudaEventRecord(out_done[0], ctx->stream));
+    CTB_CUDA(ctx, cudaEventRecord(out_done[1], ctx->stream));
+    for (int k = 0; k < nslab; ++k) {
+        const int b = k & 1;
+        const int z0 = k * slab, nz = std::min(slab, depth - z0);
+        const size_t off = static_cast<size_t>(z0) * n * n, cnt = static_cast<size_t>(nz) * n * n;
+        float* in_b = d_in + b * per;
+        float* out_b = d_out + b * per;
+        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_in, computed[b], 0));  // slab k - 2 no longer reads in_b
+        CTB_CUDA(ctx, cudaMemcpyAsync(in_b, vol + off, cnt * sizeof(float), cudaMemcpyHostToDevice, ctx->copy_in));
+        CTB_CUDA(ctx, cudaEventRecord(in_done[b], ctx->copy_in));
+        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, in_done[b], 0));
+        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, out_done[b], 0));  // slab k - 2 copied out of out_b
+        CTB_CUDA(ctx, cudaEventRecord(t[3 * k], ctx->stream));
+        CTB_TRY(forward_stage(ctx, in_b, n, n, nz, num_angles, detector_bins, nullptr, d_sino, d_stats, nullptr,
+                              true));
+        CTB_CUDA(ctx, cudaEventRecord(t[3 * k + 1], ctx->stream));
+        CTB_TRY(fbp_stage(ctx, d_sino, nz, num_angles, detector_bins, nullptr, n, filter, d_stats,
+                          ctx->convention == kConvCuda ? CTB_DENORM_CUDA : CTB_DENORM_SERIAL, out_b, nullptr,
+                          depth));
+        CTB_CUDA(ctx, cudaEventRecord(t[3 * k + 2], ctx->stream));
+        CTB_CUDA(ctx, cudaEventRecord(computed[b], ctx->stream));
+        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, computed[b], 0));
+        CTB_CUDA(ctx, cudaMemcpyAsync(out + off, out_b, cnt * sizeof(float), cudaMemcpyDeviceToHost, ctx->copy_out));
+        CTB_CUDA(ctx, cudaEventRecord(out_done[b], ctx->copy_out));
+    }
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->copy_out));
     CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    float a = 0.f, b = 0.f;
-    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
-    cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
-    ctx->last_sino_ms = a;
-    ctx->last_recon_ms = b;
+    double fwd = 0.0, fbp = 0.0;
+    for (int k = 0; k < nslab; ++k) {
+        float a = 0.f, c = 0.f;
+        cudaEventElapsedTime(&a, t[3 * k], t[3 * k + 1]);
+        cudaEventElapsedTime(&c, t[3 * k + 1], t[3 * k + 2]);
+        fwd += a;
+        fbp += c;
+    }
+    ctx->last_sino_ms = fwd;
+    ctx->last_recon_ms = fbp;
     return check_error_word(ctx);
 }
 

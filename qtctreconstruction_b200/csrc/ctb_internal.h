@@ -223,6 +223,10 @@ struct ctb_ctx {
     double last_sino_ms = 0.0;
     double last_recon_ms = 0.0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // Copy streams and per-slab events of the host-buffer volume pipeline
+    // (created on first use).
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    std::vector<cudaEvent_t> slab_ev;
 
     // Named workspaces, grown on demand and kept until destruction.
     std::map<std::string, ctb::DevBuf> ws;
