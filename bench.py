@@ -486,9 +486,10 @@ def make_batch_inputs(be, torch, shapes, seed: int):
 
 def run_batch(args, cfg, rank: int, world: int, local: int):
     """Config "batch": `jobs` uneven FBP jobs from device-resident sinograms.
-    One step = every job filtered and backprojected. Timed three ways on the
+    One step = every job filtered and backprojected. Timed four ways on the
     same jobs: the batch replayed from a CUDA graph (the value), the batch
-    launched directly, and one filter + one backprojection launch per job."""
+    launched directly, the batch with its backprojection on the persistent work
+    queue, and one filter + one backprojection launch per job."""
     import torch
 
     import qtctreconstruction_b200 as ctb
@@ -501,7 +502,8 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
     jobs, keep = make_batch_inputs(be, torch, shapes, cfg["seed"])
     updates = sum(s["n"] ** 2 * s["nz"] * s["na"] for s in shapes)
     results, outputs = {}, {}
-    for mode, flags in (("graph", ctb.BATCH_GRAPH), ("direct", 0), ("per_job", ctb.BATCH_PER_JOB)):
+    for mode, flags in (("graph", ctb.BATCH_GRAPH), ("direct", 0),
+                        ("persistent", ctb.BATCH_GRAPH | ctb.BATCH_PERSISTENT), ("per_job", ctb.BATCH_PER_JOB)):
         with be.batch(jobs, flags) as b:
             launches, _, nbytes = b.info()
             for _ in range(args.warmup):
@@ -521,7 +523,7 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
             if sampler:
                 results[mode]["clocks"] = sampler.stop()
             outputs[mode] = [o.sum().item() for _, o in keep[:4]]
-    same = outputs["graph"] == outputs["direct"] == outputs["per_job"]
+    same = outputs["graph"] == outputs["direct"] == outputs["persistent"] == outputs["per_job"]
     g = results["graph"]
     line = {
         "metric": METRIC, "value": g["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,

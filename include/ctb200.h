@@ -273,15 +273,18 @@ typedef struct ctb_batch ctb_batch;
 
 enum {
     CTB_BATCH_GRAPH = 1,    /* capture the launches once as a CUDA graph; ctb_batch_run replays it */
-    CTB_BATCH_PER_JOB = 2   /* one filter + one backprojection launch per job (comparison mode) */
+    CTB_BATCH_PER_JOB = 2,  /* one filter + one backprojection launch per job (comparison mode) */
+    CTB_BATCH_PERSISTENT = 4 /* backprojection on a persistent grid drawing (job, slice group, tile)
+                                items from an atomic counter instead of one CTA per item */
 };
 
 /* Plan a batch: device state for every job (angle tables, filtered rows) is
  * allocated here, jobs are grouped by convolution length, and the work of all
- * jobs shares one filter launch per length class and one persistent
- * backprojection launch (a work queue of (job, slice group, tile) items,
- * longest jobs first). The batch keeps the job pointers; it must be destroyed
- * before its context. */
+ * jobs shares one filter launch per length class and one backprojection launch
+ * per tile shape over the (job, slice group, tile) items, longest jobs first
+ * (one CTA per item by default, a persistent work queue with
+ * CTB_BATCH_PERSISTENT). The batch keeps the job pointers; it must be
+ * destroyed before its context. */
 ctb_status ctb_batch_create(ctb_ctx* ctx, const ctb_fbp_job* jobs, int njobs, int flags,
                             ctb_batch** out);
 /* Enqueue the batch on the context's stream (asynchronous). */

@@ -110,6 +110,7 @@ FILTER_MODE_FFT = 0         # CTB_FILTER_MODE_FFT
 FILTER_MODE_TC_BF16X3 = 1   # CTB_FILTER_MODE_TC_BF16X3
 BATCH_GRAPH = 1    # CTB_BATCH_GRAPH
 BATCH_PER_JOB = 2  # CTB_BATCH_PER_JOB
+BATCH_PERSISTENT = 4  # CTB_BATCH_PERSISTENT
 
 
 def library() -> ctypes.CDLL:
@@ -764,6 +765,6 @@ GENERATOR3D_TISSUE = np.array(
     [-20.0, 45.0, 3.0, 10.0, 0.0, 0.0, 0.0, 1.0,
      200.0, 1000.0, 2.0, 8.0, 1.0, 0.7, 0.9, 0.15], dtype=np.float32)
 
-__all__ = ["CONVENTION_SERIAL", "CONVENTION_CUDA", "bp_shape_info", "load_sinogram_file", "save_sinogram_file", "FILTER_MODE_FFT", "FILTER_MODE_TC_BF16X3", "B200Backend", "Batch", "Server", "Arena", "ServerConfig", "Request", "ServerStats", "REQ_DEVICE", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
+__all__ = ["CONVENTION_SERIAL", "CONVENTION_CUDA", "bp_shape_info", "load_sinogram_file", "save_sinogram_file", "FILTER_MODE_FFT", "FILTER_MODE_TC_BF16X3", "B200Backend", "Batch", "Server", "Arena", "ServerConfig", "Request", "ServerStats", "REQ_DEVICE", "FbpJob", "BATCH_GRAPH", "BATCH_PER_JOB", "BATCH_PERSISTENT", "FilterType", "Denorm", "ReconstructionParams", "Sinogram", "CtbError",
            "library", "pad_geometry", "filter_response", "uniform_angles_deg", "odd_detector_count",
            "phantom_params", "GENERATOR3D_TISSUE", "LIB_PATH"]

@@ -295,9 +295,11 @@ __device__ __forceinline__ bool bp_tile(BpSmem<C>& S, const BpJob& J, int zg, in
     return true;
 }
 
-// PERSISTENT = false: one CTA per item (item = blockIdx.x). Otherwise a
-// persistent grid whose thread 0 draws items from *counter.
-template <class C, bool PERSISTENT>
+// MODE 0: one job, one CTA per item (job 0 indexed statically keeps its fields
+// constant-bank operands). MODE 1: many jobs, one CTA per item, the job found
+// from blockIdx.x. MODE 2: a persistent grid whose thread 0 draws items from
+// *counter.
+template <class C, int MODE>
 __global__ void __launch_bounds__(THREADS, C::MINB) k_backproject(const __grid_constant__ BpBatch batch,
                                                                   unsigned* __restrict__ counter,
                                                                   unsigned* __restrict__ err) {
@@ -309,13 +311,23 @@ __global__ void __launch_bounds__(THREADS, C::MINB) k_backproject(const __grid_c
         mbar_fence_init();
     }
     unsigned chunks = 0;
-    if (!PERSISTENT) {
-        // one item per CTA; job 0 indexed statically keeps its fields
-        // constant-bank operands instead of registers
+    if (MODE == 0) {
         __syncthreads();
         const BpJob& J = batch.job[0];
         const int zg = blockIdx.x / J.tiles;
         const int tl = blockIdx.x - zg * J.tiles;
+        bp_tile<C>(S, J, zg, (tl % J.tiles_x) * C::TX, (tl / J.tiles_x) * C::TY, chunks, err);
+        return;
+    }
+    if (MODE == 1) {
+        __syncthreads();
+        const int item = blockIdx.x;
+        int j = 0;
+        while (j + 1 < batch.njobs && batch.job[j + 1].first <= item) ++j;
+        const BpJob& J = batch.job[j];
+        const int local = item - static_cast<int>(J.first);
+        const int zg = local / J.tiles;
+        const int tl = local - zg * J.tiles;
         bp_tile<C>(S, J, zg, (tl % J.tiles_x) * C::TX, (tl / J.tiles_x) * C::TY, chunks, err);
         return;
     }
@@ -337,33 +349,39 @@ __global__ void __launch_bounds__(THREADS, C::MINB) k_backproject(const __grid_c
 
 template <class C>
 cudaError_t set_smem() {
-    cudaError_t e = cudaFuncSetAttribute(k_backproject<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(sizeof(BpSmem<C>)));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_backproject<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(sizeof(BpSmem<C>)));
+    const int bytes = static_cast<int>(sizeof(BpSmem<C>));
+    cudaError_t e = cudaFuncSetAttribute(k_backproject<C, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_backproject<C, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_backproject<C, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
 }
 
 template <class C>
 cudaError_t launch_one(const BpBatch& b, unsigned* d_err, cudaStream_t st) {
     cudaError_t e = set_smem<C>();
     if (e != cudaSuccess) return e;
-    k_backproject<C, false><<<static_cast<unsigned>(b.total), THREADS, sizeof(BpSmem<C>), st>>>(b, nullptr, d_err);
+    k_backproject<C, 0><<<static_cast<unsigned>(b.total), THREADS, sizeof(BpSmem<C>), st>>>(b, nullptr, d_err);
     return cudaGetLastError();
 }
 
 template <class C>
-cudaError_t launch_persistent(const BpBatch& b, unsigned* d_counter, unsigned* d_err, cudaStream_t st) {
+cudaError_t launch_many(const BpBatch& b, bool persistent, unsigned* d_counter, unsigned* d_err, cudaStream_t st) {
     cudaError_t e = set_smem<C>();
     if (e != cudaSuccess) return e;
+    if (!persistent) {
+        k_backproject<C, 1><<<static_cast<unsigned>(b.total), THREADS, sizeof(BpSmem<C>), st>>>(b, nullptr, d_err);
+        return cudaGetLastError();
+    }
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backproject<C, true>, THREADS, sizeof(BpSmem<C>));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backproject<C, 2>, THREADS, sizeof(BpSmem<C>));
     const long long grid = std::min<long long>(b.total, static_cast<long long>(sms) * (per_sm > 0 ? per_sm : 1));
     e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
-    k_backproject<C, true><<<static_cast<unsigned>(grid), THREADS, sizeof(BpSmem<C>), st>>>(b, d_counter, d_err);
+    k_backproject<C, 2><<<static_cast<unsigned>(grid), THREADS, sizeof(BpSmem<C>), st>>>(b, d_counter, d_err);
     return cudaGetLastError();
 }
 
@@ -445,14 +463,14 @@ BpJob make_bp_job(const float4* d_filt, int nz, int na, const FiltLayout& fl, in
 }
 
 cudaError_t launch_backproject_batch(const BpBatch& b, int variant, unsigned* d_counter, unsigned* d_err,
-                                     cudaStream_t st) {
+                                     cudaStream_t st, bool persistent) {
     if (b.total == 0) return cudaSuccess;
     if (b.total > 0x7fffffffLL) return cudaErrorInvalidValue;
     switch (variant) {
-    case 1: return launch_persistent<V1>(b, d_counter, d_err, st);
-    case 2: return launch_persistent<V2>(b, d_counter, d_err, st);
-    case 3: return launch_persistent<V3>(b, d_counter, d_err, st);
-    default: return launch_persistent<V0>(b, d_counter, d_err, st);
+    case 1: return launch_many<V1>(b, persistent, d_counter, d_err, st);
+    case 2: return launch_many<V2>(b, persistent, d_counter, d_err, st);
+    case 3: return launch_many<V3>(b, persistent, d_counter, d_err, st);
+    default: return launch_many<V0>(b, persistent, d_counter, d_err, st);
     }
 }
 

@@ -68,7 +68,8 @@ ctb_status issue(ctb_batch* b) {
             CTB_LAUNCH(ctx, launch_backproject(J.filt, J.nz, J.na, fl, J.n, J.trig, nullptr,
                                                CTB_DENORM_NONE, J.out, ctx->d_err, ctx->stream, v));
         } else {
-            CTB_LAUNCH(ctx, launch_backproject_batch(p, v, b->d_counter, ctx->d_err, ctx->stream));
+            CTB_LAUNCH(ctx, launch_backproject_batch(p, v, b->d_counter, ctx->d_err, ctx->stream,
+                                                     (b->flags & CTB_BATCH_PERSISTENT) != 0));
         }
     }
     return CTB_OK;
@@ -211,7 +212,7 @@ ctb_status ctb_batch_create(ctb_ctx* ctx, const ctb_fbp_job* jobs, int njobs, in
                             ctb_batch** out) {
     if (!ctx || !out) return CTB_ERR_INVALID;
     *out = nullptr;
-    if (!jobs || njobs <= 0 || (flags & ~(CTB_BATCH_GRAPH | CTB_BATCH_PER_JOB)))
+    if (!jobs || njobs <= 0 || (flags & ~(CTB_BATCH_GRAPH | CTB_BATCH_PER_JOB | CTB_BATCH_PERSISTENT)))
         return fail(ctx, CTB_ERR_INVALID, "ctb_batch_create: invalid arguments");
     for (int i = 0; i < njobs; ++i) CTB_TRY(check_job(ctx, jobs[i], i));
     Guard g(ctx);

@@ -190,11 +190,11 @@ BpJob make_bp_job(const float4* d_filt, int nz, int na, const FiltLayout& fl, in
 FiltJob make_filt_job(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
                       const float2* d_Hc, const float4* d_stats, int denorm, float scale,
                       float4* d_filt);
-// Backprojection of a batch (below 2^31 items) on a persistent grid: d_counter
-// (zeroed here on the stream) hands out the items. Filtering takes one CTA per
-// item.
+// Backprojection of a batch (below 2^31 items, one tile shape): one CTA per
+// item, or with `persistent` a grid of resident CTAs drawing items from
+// d_counter (zeroed here on the stream). Filtering takes one CTA per item.
 cudaError_t launch_backproject_batch(const BpBatch& b, int variant, unsigned* d_counter, unsigned* d_err,
-                                     cudaStream_t st);
+                                     cudaStream_t st, bool persistent = false);
 cudaError_t launch_filter_batch(const FiltBatch& b, cudaStream_t st);
 cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltLayout& fl,
                                int n_out, Trig trig, const float4* d_stats, int denorm,

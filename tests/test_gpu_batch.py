@@ -2,7 +2,8 @@
 
 A job's result must not depend on the batch: it is compared bit for bit with
 ctb_fbp_d on the same job alone, with the job alone in a batch, in a mixed
-batch, in the per-job launch mode and replayed from a CUDA graph. One job per
+batch, in the per-job launch mode, on the persistent work queue and replayed
+from a CUDA graph. One job per
 batch is also checked against the oracle (SerialBackend's float path) within
 the parity tolerance rel-L2 <= 1e-5, max-abs <= 1e-4 * max|f|.
 """
@@ -85,7 +86,8 @@ def test_alone_vs_mixed_and_modes(backend):
         backend.synchronize()
     alone = host[target]["d_out"].cpu().numpy().copy()
     results = {}
-    for flags in (0, ctb.BATCH_GRAPH, ctb.BATCH_PER_JOB, ctb.BATCH_GRAPH | ctb.BATCH_PER_JOB):
+    for flags in (0, ctb.BATCH_GRAPH, ctb.BATCH_PER_JOB, ctb.BATCH_GRAPH | ctb.BATCH_PER_JOB, ctb.BATCH_PERSISTENT,
+                  ctb.BATCH_GRAPH | ctb.BATCH_PERSISTENT):
         for h in host:
             h["d_out"].fill_(float("nan"))
         with backend.batch(jobs, flags) as b:
