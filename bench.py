@@ -216,6 +216,27 @@ def cpu_reference_rate(cfg: dict, slices: int, params, repeats: int = 1):
     return n * n * slices * na / best, threads, "reference", isa, sample
 
 
+def cpu_native_rate(cfg: dict, slices: int, params):
+    """The reference OpenMPBackend's own reconstructVolume (its native volume
+    path: detector bins = N, symmetric-z SIMD backprojection) on `slices`
+    slices of the phantom, all host threads. Returns (updates/s, threads) or
+    None when the reference build is absent."""
+    import oracle as O
+    from oracle import reference as R
+    lib, _ = R.timing_lib()
+    if lib is None:
+        return None
+    n, nz, na, kind = cfg["n"], cfg["nz"], cfg["na"], cfg["filter"]
+    vol = O.phantom_sum_slab(params, n, n, nz, nz // 2 - slices // 2, slices)
+    threads = os.cpu_count() or 1
+    lib.ref_set_threads(threads)
+    R.reconstruct_volume(R.OPENMP, vol[:2], na, kind, lib=lib)  # warm-up
+    t0 = time.perf_counter()
+    R.reconstruct_volume(R.OPENMP, vol, na, kind, lib=lib)
+    dt = time.perf_counter() - t0
+    return n * n * slices * na / dt, threads
+
+
 def run_reference(args, cfg, rank: int, world: int):
     """--impl reference: the reference's CPU path, rank 0 only."""
     if rank != 0:
@@ -376,6 +397,12 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
             r, threads, kind_b, isa, sample = cpu_reference_rate(cfg, args.ref_slices, params)
             line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": threads, "kind": kind_b,
                                     "sample": sample}
+            nat = cpu_native_rate(cfg, 4 * args.ref_slices, params)
+            if nat:
+                line["cpu_baseline_native"] = {
+                    "value": nat[0], "unit": UNIT, "cores": nat[1], "kind": "reference",
+                    "sample": f"{4 * args.ref_slices} of {cfg['nz']} slices, OpenMPBackend::reconstructVolume "
+                              "(its native volume path, detector bins = N)"}
         print(json.dumps(line), flush=True)
     be.close()
     if dist is not None:
