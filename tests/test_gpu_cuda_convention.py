@@ -93,3 +93,16 @@ def test_convention_switch_leaves_serial_unchanged(backend, golden):
     np.testing.assert_array_equal(backend.computeSinogram(golden["cfg_like_slice"], na, nd).data, a)
     with pytest.raises(ctb.CtbError):
         backend.set_convention(5)
+
+
+def test_non_square_sinogram_against_fp64(cuda_be):
+    rng = np.random.default_rng(8)
+    w, h, na, nd = 90, 52, 70, 107
+    s = np.zeros((h, w), np.float32)
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    for _ in range(4):
+        cx, cy = rng.uniform(0.3 * w, 0.7 * w), rng.uniform(0.3 * h, 0.7 * h)
+        s[((xx - cx) / 9.0) ** 2 + ((yy - cy) / 6.0) ** 2 <= 1.0] += np.float32(rng.uniform(50, 500))
+    sino = cuda_be.computeSinogram(s, na, nd)
+    f64, _, _ = O.cc_sinogram_f64(s, na, nd)
+    _close(sino.data, f64)

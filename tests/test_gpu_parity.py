@@ -252,3 +252,36 @@ def test_host_volume_pipeline_equals_device_path(backend):
     np.testing.assert_array_equal(host, d_out.cpu().numpy())
     ser = O.reconstruct_volume_f32(vol[:6], na, nd, O.SHEPP_LOGAN)
     _close(host[:6], ser)
+
+
+@pytest.mark.parametrize("w,h", [(80, 48), (37, 101)])
+def test_sinogram_non_square_slice(backend, w, h):
+    """computeSinogram takes any width x height (SerialBackend.cpp:59-136):
+    the walked axis and its transposed copy differ in length."""
+    rng = np.random.default_rng(w * h)
+    sl = np.zeros((h, w), np.float32)
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    for _ in range(4):
+        cx, cy = rng.uniform(0.3 * w, 0.7 * w), rng.uniform(0.3 * h, 0.7 * h)
+        a, b = rng.uniform(0.05, 0.2) * w, rng.uniform(0.05, 0.2) * h
+        sl[((xx - cx) / a) ** 2 + ((yy - cy) / b) ** 2 <= 1.0] += np.float32(rng.uniform(0.2, 1.0))
+    na, nd = 90, ctb.odd_detector_count(max(w, h))
+    gpu = backend.computeSinogram(sl, na, nd)
+    ref, ang, mm = O.sinogram_f32(sl, na, nd)
+    _close(gpu.data, ref)
+    assert (gpu.original_min_hu, gpu.original_max_hu) == (mm[0], mm[1])
+    f64, _ = O.sinogram_f64(sl, na, nd, ang)
+    assert O.rel_l2(gpu.data, f64) <= O.rel_l2(ref, f64)  # at least as accurate as SerialBackend
+
+
+def test_angles_outside_half_turn_and_single_angle(backend):
+    rng = np.random.default_rng(21)
+    n = 64
+    nd = ctb.odd_detector_count(n)
+    sl = ellipse_slice(rng, n, 4)
+    for ang in (np.sort(rng.uniform(-90, 300, 61)).astype(np.float32), np.float32([37.5])):
+        s64, _ = O.sinogram_f64(sl, len(ang), nd, ang)
+        s32 = s64.astype(np.float32)
+        ser = O.reconstruct_slice_f32(s32, ang, n, O.RAMP)
+        gpu = backend.reconstructSlice(ctb.Sinogram(s32, ang), n, ReconstructionParams(FilterType.Ramp, len(ang)))
+        _close(gpu, ser)

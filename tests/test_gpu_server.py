@@ -142,3 +142,27 @@ def test_shutdown_with_queued_work():
     ids = [srv.submit(r["sino"], r["n"], r["kind"]) for r in reqs]
     assert srv.wait(ids[0]) == OK
     srv.close()  # cancels what is still queued and returns
+
+
+def test_concurrent_submitters(backend):
+    """Requests submitted from several host threads at once all complete and
+    each equals the request alone."""
+    import threading
+
+    import torch
+    reqs = _requests(SHAPES * 2, 27)
+    with ctb.Server(0, memory_budget=1 << 30, copy_threads=3) as srv:
+        ids = [None] * len(reqs)
+
+        def submit(k0):
+            for k in range(k0, len(reqs), 4):
+                r = reqs[k]
+                ids[k] = srv.submit(r["sino"], r["n"], r["kind"], angles_deg=r["angles"])
+        th = [threading.Thread(target=submit, args=(k,)) for k in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        outs = [srv.result(i) for i in ids]
+    for r, o in zip(reqs, outs):
+        np.testing.assert_array_equal(o, _alone(backend, torch, r))
