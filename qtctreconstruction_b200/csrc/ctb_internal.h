@@ -89,18 +89,18 @@ cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const flo
 // normalised image planes (img only).
 cudaError_t launch_raymarch(const float4* d_img, int w, int h, int nz, int na, int nd, float det_center,
                             const double2* d_cs, float* d_sino, cudaStream_t st);
-// Forward projector work plan: angles grouped (up to kFwdGroup per CTA) by
-// walked axis so that one staged row segment of kFwdWidth pixels serves every
-// angle of the group. groups: {first index into order, count, axis (0 rows,
-// 1 columns), 0}.
-constexpr int kFwdRays = 128;   // rays (detector bins) per CTA
-constexpr int kFwdRows = 8;     // walked rows per staged chunk
-constexpr int kFwdWidth = 256;  // staged pixels per row
-constexpr int kFwdGroup = 4;    // angles per CTA
+// Forward projector work plan: angles grouped (up to kFwdGroup per CTA, in
+// their given order) by walked axis, so that the angles of a CTA read the
+// same image rows at the same time. groups: {first index into order, count,
+// axis (0 rows, 1 columns), 0}.
+constexpr int kFwdRays = 128;  // detector intervals per CTA (kFwdRays - 1 output bins)
+constexpr int kFwdRows = 8;    // walked rows per chunk (boundaries in double once per chunk)
+constexpr int kFwdGroup = 4;   // angles per CTA
+constexpr int kFwdPlanes = 2;  // float4 image planes (4 slices each) per thread
 // Zero border of the normalised image planes: kFwdGuard pixels on both sides
-// of every row (>= kFwdWidth + reach) and kFwdRows rows after the last, so a
-// staged segment never leaves the plane.
-constexpr int kFwdGuard = 264;
+// of every row and kFwdRows rows after the last, so that every chunk the
+// projector walks reads inside the plane.
+constexpr int kFwdGuard = 16;
 inline size_t fwd_plane_elems(int np, int nq) {
     return static_cast<size_t>(np + kFwdRows) * static_cast<size_t>(nq + 2 * kFwdGuard);
 }

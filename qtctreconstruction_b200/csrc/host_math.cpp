@@ -228,54 +228,25 @@ namespace ctb {
 
 // Group the projection angles for the forward projector: angles are split by
 // walked axis (|cos| >= |sin| walks rows, else columns), kept in their given
-// order within each axis, and packed greedily into groups of up to kFwdGroup
-// angles whose staged row segment provably fits kFwdWidth pixels. For fixed
-// (b, p) the crossing is q*(b, p) = cq + (b - dcf) inv + (p - cp) dq with
-// inv = 1/kq and dq = -kp/kq; over a CTA's kFwdRays bins and a chunk's
-// kFwdRows rows one angle spans at most (kFwdRays-1)|inv| + (kFwdRows-1)|dq|
-// pixels, and two angles of a group differ by at most
-// Bmax |inv_i - inv_j| + Pmax |dq_i - dq_j| at any (b, p).
+// order within each axis, and cut into groups of kFwdGroup consecutive
+// angles, which walk nearly the same rows and columns and so share L1 lines.
 FwdPlan forward_plan(const float* angles_deg, int na, int w, int h, int nd) {
-    struct Ang {
-        int a;
-        double inv, dq;
-    };
-    std::vector<Ang> lists[2];
+    (void)w;
+    (void)h;
+    (void)nd;
+    std::vector<int> lists[2];
     for (int a = 0; a < na; ++a) {
         const double th = static_cast<double>(angles_deg[a]) * 3.14159265358979323846 / 180.0;
-        const double c = std::cos(th), s = std::sin(th);
-        const int axis = std::fabs(c) >= std::fabs(s) ? 0 : 1;
-        const double kq = axis == 0 ? c : s, kp = axis == 0 ? s : c;
-        lists[axis].push_back({a, 1.0 / kq, -kp / kq});
+        lists[std::fabs(std::cos(th)) >= std::fabs(std::sin(th)) ? 0 : 1].push_back(a);
     }
-    const double dcf = nd / 2;
-    const double bmax = std::max(dcf, nd - 1 - dcf);
     FwdPlan plan;
     for (int axis = 0; axis < 2; ++axis) {
-        const int np = axis == 0 ? h : w;
-        const double cp = 0.5 * (np - 1);
-        const double pmax = std::max(cp, np - 1 - cp);
         const auto& L = lists[axis];
-        size_t i = 0;
-        while (i < L.size()) {
+        for (size_t i = 0; i < L.size(); i += kFwdGroup) {
             const int first = static_cast<int>(plan.order.size());
-            double imin = L[i].inv, imax = L[i].inv, dmin = L[i].dq, dmax = L[i].dq;
-            double amax = std::fabs(L[i].inv), qmax = std::fabs(L[i].dq);
-            plan.order.push_back(L[i].a);
-            size_t j = i + 1;
-            for (; j < L.size() && static_cast<int>(j - i) < kFwdGroup; ++j) {
-                const double ni = std::min(imin, L[j].inv), xi = std::max(imax, L[j].inv);
-                const double nq = std::min(dmin, L[j].dq), xq = std::max(dmax, L[j].dq);
-                const double na_ = std::max(amax, std::fabs(L[j].inv));
-                const double nqq = std::max(qmax, std::fabs(L[j].dq));
-                const double need = (kFwdRays - 1) * na_ + (kFwdRows - 1) * nqq +
-                                    bmax * (xi - ni) + pmax * (xq - nq) + 10.0;
-                if (need > kFwdWidth) break;
-                imin = ni; imax = xi; dmin = nq; dmax = xq; amax = na_; qmax = nqq;
-                plan.order.push_back(L[j].a);
-            }
-            plan.groups.insert(plan.groups.end(), {first, static_cast<int>(j - i), axis, 0});
-            i = j;
+            const int cnt = static_cast<int>(std::min<size_t>(kFwdGroup, L.size() - i));
+            for (int k = 0; k < cnt; ++k) plan.order.push_back(L[i + k]);
+            plan.groups.insert(plan.groups.end(), {first, cnt, axis, 0});
         }
     }
     return plan;
