@@ -93,14 +93,14 @@ cudaError_t launch_raymarch(const float4* d_img, int w, int h, int nz, int na, i
 // their given order) by walked axis, so that the angles of a CTA read the
 // same image rows at the same time. groups: {first index into order, count,
 // axis (0 rows, 1 columns), 0}.
-constexpr int kFwdRays = 128;  // detector intervals per CTA (kFwdRays - 1 output bins)
-constexpr int kFwdRows = 8;    // walked rows per chunk (boundaries in double once per chunk)
+constexpr int kFwdRays = 32;   // detector intervals per CTA (kFwdRays - 1 output bins)
+constexpr int kFwdRows = 16;   // walked rows per chunk (boundaries in double once per chunk)
 constexpr int kFwdGroup = 4;   // angles per CTA
 constexpr int kFwdPlanes = 2;  // float4 image planes (4 slices each) per thread
 // Zero border of the normalised image planes: kFwdGuard pixels on both sides
 // of every row and kFwdRows rows after the last, so that every chunk the
 // projector walks reads inside the plane.
-constexpr int kFwdGuard = 16;
+constexpr int kFwdGuard = kFwdRows + 8;
 inline size_t fwd_plane_elems(int np, int nq) {
     return static_cast<size_t>(np + kFwdRows) * static_cast<size_t>(nq + 2 * kFwdGuard);
 }

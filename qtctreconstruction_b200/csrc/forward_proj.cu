@@ -16,20 +16,22 @@
 // when |cos| >= |sin|, else columns of the transposed copy), so an interval
 // holds one or two pixels of each walked row. Its two boundaries (the
 // crossings of bins j and j+1) are evaluated in double once per chunk of
-// PCH = 8 rows as an integer column plus a float offset, and stepped in float
+// PCH = 16 rows as an integer column plus a float offset, and stepped in float
 // within the chunk; threads that share a boundary evaluate it identically, so
 // membership (an exact comparison of a pixel column with a boundary) gives a
 // partition of the pixels. The two edge intervals (0 and nd-1), where the
 // reference's rules are discontinuous, decide membership on the reference's
 // own float s (SerialBackend.cpp:109-120) on a separate, warp-uniform path.
 //
-// A CTA owns FB = 128 consecutive intervals (FB - 1 output bins), one group
-// of up to GMAX = 4 angles that share the walked axis (thread (x, y): interval
-// x, angle y) and 4 NP slices (NP float4 planes of the normalised image).
-// Pixels are read straight from the zero-bordered planes through L1 (the 4
-// angles of a CTA read the same rows at the same time); warps walk their own
-// row ranges independently, with no staging and no CTA-wide waits.
-// Accumulation runs on packed FP32x2 instructions.
+// A CTA is one warp per angle of a group of up to GMAX = 4 angles that share
+// the walked axis; lane x of every warp owns interval jb + x of FB = 32
+// consecutive intervals (FB - 1 output bins, the last interval only feeds the
+// neighbour sum), for 4 NP slices (NP float4 planes of the normalised image).
+// Pixels are read straight from the zero-bordered planes through L1: the
+// warps of a CTA walk nearly the same rows at the same time and share the
+// lines. Warps never wait on one another, and the CTA's warps have nearly
+// equal row counts, so CTAs retire evenly. Accumulation runs on packed FP32x2
+// instructions.
 #include <cmath>
 
 #include "ctb_internal.h"
@@ -37,8 +39,9 @@
 namespace ctb {
 namespace {
 
-constexpr int FB = kFwdRays;  // intervals per CTA
+constexpr int FB = kFwdRays;  // intervals per CTA (one warp per angle)
 constexpr int OUT = FB - 1;   // output bins per CTA
+static_assert(FB == 32, "a warp owns the CTA's intervals of one angle");
 constexpr int PCH = kFwdRows;
 constexpr int GMAX = kFwdGroup;
 constexpr int AY = GMAX;  // angle lanes per CTA
@@ -77,16 +80,19 @@ __device__ __forceinline__ Bound boundary(const FAngle& f, int t, int p0) {
     return Bound{static_cast<int>(qfl), static_cast<float>(qstar - qfl)};
 }
 
-// Reads stay inside the zero-bordered plane (kFwdGuard = 16 columns each
-// side): within [4 - kFwdGuard, nq + kFwdGuard - 4] every candidate column is
-// inside the border. A boundary that leaves that range at some row of the
-// chunk is more than 12 columns outside the image there, and since it moves
-// at most one column per row and its interval is at most sqrt 2 wide, the
-// interval holds only zero pixels for the whole chunk, which is skipped.
-__device__ __forceinline__ bool chunk_inside(const Bound& b, float dqf, int nq) {
-    const float lq = static_cast<float>(b.base) + b.f;
-    return lq + fminf(0.0f, (PCH - 1) * dqf) >= static_cast<float>(4 - kFwdGuard) &&
-           lq + fmaxf(0.0f, (PCH - 1) * dqf) <= static_cast<float>(nq + kFwdGuard - 4);
+// A chunk is skipped exactly when both boundaries lie left of column -2, or
+// right of column nq + 1, at its first and last rows: the boundaries are
+// linear in the row, so the interval (at most sqrt 2 wide) then holds no image
+// pixel at any row of the chunk. Otherwise some boundary is within two columns
+// of the image at some row; moving at most one column per row, every
+// candidate column of the chunk stays within kFwdRows + 5 columns of the
+// image, inside the zero border (kFwdGuard = kFwdRows + 8).
+__device__ __forceinline__ bool chunk_meets_image(const Bound& ba, const Bound& bb, float dqf, int nq) {
+    const float e = (PCH - 1) * dqf;
+    const float a0 = static_cast<float>(ba.base) + ba.f, b0 = static_cast<float>(bb.base) + bb.f;
+    const float lo = fminf(fminf(a0, a0 + e), fminf(b0, b0 + e));
+    const float hi = fmaxf(fmaxf(a0, a0 + e), fmaxf(b0, b0 + e));
+    return hi >= -2.0f && lo <= static_cast<float>(nq + 1);
 }
 
 __device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
@@ -189,14 +195,13 @@ __device__ __noinline__ Sums splat_rows_edge(const float4* __restrict__ rowp, lo
     return acc;
 }
 
-__global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict__ img,
+__global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict__ img,
                                                         const float4* __restrict__ imgT, int w,
                                                         int h, int nz, int na, int nd, Trig trig,
                                                         const int4* __restrict__ groups,
                                                         const int* __restrict__ order,
                                                         float* __restrict__ sino) {
     __shared__ FAngle fa[GMAX];
-    __shared__ float2 xl[AY][FB / 32][2 * NP];  // left parts of each warp's first interval
 
     const int ob0 = blockIdx.x * OUT;  // first output bin of the CTA
     const int nout = min(OUT, nd - ob0);
@@ -205,9 +210,8 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     const int4 grp = groups[blockIdx.y];
     const int cnt = grp.y;
     const bool rows = grp.z == 0;
-    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // tx: lane (interval), ty: warp (angle)
     const int tid = ty * FB + tx;
-    const int lane = tid & 31;
     const int j = jb + tx;
 
     const int np = rows ? h : w;  // walked axis
@@ -281,19 +285,13 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     const long long pofs = g0 + 1 < ng4 ? pstride : 0;
 
     // rows this warp's intervals can touch at its angle (warp-uniform)
-    const int w0 = tx & ~31;
-    int wlo = np, whi = -1;
-    if (w0 <= nout && has_a) {
-        const FAngle& f = fa[ja];
-        prange(f.q0 + w0 * f.inv, f.q0 + min(w0 + 32, tmax) * f.inv, f.dq, wlo, whi);
-    }
+    const int wlo = has_a ? fa[ja].p_lo : 0, whi = has_a ? fa[ja].p_hi : -1;
     // interval -1 adds nothing (the reference drops floor(s) < 0); threads
     // past the CTA's last interval idle
     const bool live = has_a && tx <= nout && j >= 0;
-    // warps holding interval 0 or nd-1 at an angle where it meets the image
-    // take the reference-decision path
-    const bool holds_edge = (w0 <= -jb && -jb < w0 + 32) || (w0 <= nd - 1 - jb && nd - 1 - jb < w0 + 32);
-    const bool edge_a = holds_edge && has_a && fa[ja].edge;
+    // a warp holding interval 0 or nd-1 at an angle where it meets the image
+    // takes the reference-decision path
+    const bool edge_a = has_a && fa[ja].edge;
     const bool neg = has_a && fa[ja].neg;
     const float cxf = static_cast<float>(w - 1) * 0.5f, cyf = static_cast<float>(h - 1) * 0.5f;
 
@@ -305,7 +303,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
         for (int p0 = wlo; p0 <= whi; p0 += PCH) {
             const Bound ba = boundary(f, tx, p0);
             const Bound bb = boundary(f, tx + 1, p0);
-            if (!chunk_inside(ba, f.dqf, nq) || !chunk_inside(bb, f.dqf, nq)) continue;
+            if (!chunk_meets_image(ba, bb, f.dqf, nq)) continue;
             const float4* rowp = plane + static_cast<long long>(p0) * pitch;
             if (edge_a) acc = splat_rows_edge(rowp, pofs, pitch, f, ba, bb, p0, j, nd, rows, cxf, cyf, acc);
             else if (neg) splat_rows<-1>(rowp, pofs, pitch, ba, bb, f.dqf, acc.v, acc.d);
@@ -315,19 +313,13 @@ __global__ void __launch_bounds__(THREADS, 2) k_forward(const float4* __restrict
     // bin jb + x + 1 = frac part of interval x + (1 - frac) part of interval x + 1
     const float akq = has_a ? fa[ja].akq : 0.0f;
     const float2 ak = make_float2(akq, akq);
-    float2 right[2 * NP], left[2 * NP], nxt[2 * NP];
+    float2 right[2 * NP], nxt[2 * NP];
 #pragma unroll
     for (int k = 0; k < 2 * NP; ++k) {
         right[k] = __fmul2_rn(ak, acc.d[k]);
-        left[k] = make_float2(acc.v[k].x - right[k].x, acc.v[k].y - right[k].y);
-        if (lane == 0) xl[ty][tx >> 5][k] = left[k];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 2 * NP; ++k) {
-        nxt[k].x = __shfl_down_sync(0xffffffffu, left[k].x, 1);
-        nxt[k].y = __shfl_down_sync(0xffffffffu, left[k].y, 1);
-        if (lane == 31 && tx + 1 < FB) nxt[k] = xl[ty][(tx + 1) >> 5][k];
+        const float2 left = make_float2(acc.v[k].x - right[k].x, acc.v[k].y - right[k].y);
+        nxt[k].x = __shfl_down_sync(0xffffffffu, left.x, 1);
+        nxt[k].y = __shfl_down_sync(0xffffffffu, left.y, 1);
     }
     if (!outs) return;
     const long long ob = static_cast<long long>(fa[ja].a) * nd + ob0 + tx;
