@@ -68,7 +68,7 @@ struct FAngle {
 // of the chunk crosses at base + (f + pp dq). Every thread that needs
 // boundary t evaluates exactly this expression on the same operands, so the
 // two threads sharing a boundary hold the same integer and the same floats.
-// The float stays below |dq| (PCH - 1) + 1, where its rounding is ~30x finer
+// The float stays below |dq| (PCH - 1) + 1, where its rounding is ~16x finer
 // than that of a float column coordinate.
 struct Bound {
     int base;
