@@ -141,9 +141,10 @@ def gpu_id_for(device: int) -> str:
         return vis.split(",")[device] if vis else str(device)
 
 
-def load_profile_traffic(config: str):
-    """DRAM bytes per backprojection launch from the committed ncu summary (JSON text), if any."""
-    path = os.path.join(ROOT, "profiles", f"backproject_{config}_traffic.txt")
+def load_profile_traffic(kernel: str, config: str):
+    """DRAM bytes per launch of `kernel` ("forward", "backproject") from the
+    committed ncu summary (JSON text), if any."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{config}_traffic.txt")
     try:
         with open(path) as f:
             return json.load(f).get("dram_bytes_per_launch")
@@ -357,11 +358,25 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
         inside = circle_voxels(n) * nz * na
         bp_ms = float(stages[3])
         achieved = inside * 8.0 / (bp_ms * 1e-3) / 1e9  # two float taps per in-circle update
+        fwd_ms = float(stages[1])
+        fwd_achieved = 4.0 * updates / (fwd_ms * 1e-3) / 1e9  # each pixel read once per angle
         peaks = measured_peaks()
         hbm_peak = peaks.get("hbm_gbs")
         sq = math.ceil(math.sqrt(2.0) * nd)
         filt_bytes = 4.0 * (nd + sq) * nz * na
-        traffic = load_profile_traffic(args.config)
+        smem_src = "measured shared-memory load bandwidth (probe kernel, same run)"
+        roof_fwd = {"kernel": "k_forward", "bound": "l1", "achieved": fwd_achieved, "peak": smem_gbs,
+                    "unit": "GB/s", "frac": fwd_achieved / smem_gbs,
+                    "traffic": load_profile_traffic("forward", args.config),
+                    "peak_source": smem_src + "; L1 hits use the same data path",
+                    "algorithmic": "4 B (one float) per pixel-angle-slice: each pixel read once per angle"}
+        roof_bp = {"kernel": "k_backproject", "bound": "smem", "achieved": achieved,
+                   "peak": smem_gbs, "unit": "GB/s", "frac": achieved / smem_gbs,
+                   "traffic": load_profile_traffic("backproject", args.config),
+                   "peak_source": smem_src,
+                   "algorithmic": "8 B (two float taps) per in-circle voxel-angle update"}
+        # the dominant kernel of the step carries the contract's "roofline" key
+        roof_main, roof_other = (roof_fwd, roof_bp) if fwd_ms >= bp_ms else (roof_bp, roof_fwd)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -376,11 +391,8 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
                          "backproject": stages[3]},
             "fbp_only": {"value": updates / ((stages[2] + stages[3]) * 1e-3), "unit": UNIT,
                          "note": "filter + backprojection kernels only"},
-            "roofline": {"kernel": "k_backproject", "bound": "smem", "achieved": achieved,
-                         "peak": smem_gbs, "unit": "GB/s", "frac": achieved / smem_gbs,
-                         "traffic": traffic,
-                         "peak_source": "measured shared-memory load bandwidth (probe kernel, same run)",
-                         "algorithmic": "8 B (two float taps) per in-circle voxel-angle update"},
+            "roofline": roof_main,
+            "roofline_" + roof_other["kernel"][2:]: roof_other,
             "roofline_filter": {"kernel": "k_filter", "bound": "hbm",
                                 "achieved": filt_bytes / (filt_kernel_ms * 1e-3) / 1e9,
                                 "peak": hbm_peak, "unit": "GB/s",
