@@ -209,6 +209,7 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     const size_t elems = static_cast<size_t>(nzg) * std::max(fwd_plane_elems(h, w), fwd_plane_elems(w, h));
     CTB_WS(ctx, d_img, float4, "img", elems);
     CTB_WS(ctx, d_imgT, float4, "imgT", elems);
+    CTB_WS(ctx, d_box, int4, "fbox", nzg);
     // zero borders: cleared whenever the buffers or the plane geometry change
     const std::vector<long long> geom = {reinterpret_cast<long long>(d_img),
                                          reinterpret_cast<long long>(d_imgT), w, h, nzg};
@@ -219,7 +220,8 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     }
     Trig trig;
     CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
-    CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream));
+    CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream,
+                                       ctx->convention == kConvCuda ? nullptr : d_box));
     if (ctx->convention == kConvCuda) {
         CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, nullptr, ctx->stream, 0));
         mark(ctx, ev, 1);
@@ -227,13 +229,13 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
         CTB_LAUNCH(ctx, launch_raymarch(d_img, w, h, nz, na, nd, det_center, trig.cs, d_sino, ctx->stream));
         return CTB_OK;
     }
-    CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream));
+    CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream, 1, d_box));
     mark(ctx, ev, 1);
     const ctb_ctx::FwdPlanDev* plan = nullptr;
     CTB_TRY(forward_plan_dev(ctx, angles_deg, na, w, h, nd, &plan));
     CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd, trig,
                                    static_cast<const int4*>(plan->groups.ptr), plan->ngroups,
-                                   static_cast<const int*>(plan->order.ptr), d_sino, ctx->d_err,
+                                   static_cast<const int*>(plan->order.ptr), d_box, d_sino, ctx->d_err,
                                    ctx->stream));
     return CTB_OK;
 }

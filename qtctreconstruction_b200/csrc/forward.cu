@@ -2,6 +2,7 @@
 // per-slice statistics and the normalised, slice-interleaved image copies the
 // projector reads (forward_proj.cu holds the projector itself).
 #include <cfloat>
+#include <climits>
 #include <cmath>
 
 #include "ctb_internal.h"
@@ -22,9 +23,12 @@ __global__ void k_trig(const float* __restrict__ deg, int na, double2* __restric
 
 // ------------------------------------------------------------ slice stats
 // stats[z] = {min, max, span_fwd, span_denorm} (SerialBackend.cpp:70-80, 298-300).
+// With box set, also empties the non-zero bounding box of each 4-slice group
+// that k_normalize then fills.
 __global__ void __launch_bounds__(1024) k_slice_stats(const float* __restrict__ vol, long long npx,
-                                                      float4* __restrict__ stats) {
+                                                      float4* __restrict__ stats, int4* __restrict__ box) {
     const int z = blockIdx.x;
+    if (box && threadIdx.x == 0 && (z & 3) == 0) box[z >> 2] = make_int4(INT_MAX, -1, INT_MAX, -1);
     const float* p = vol + static_cast<long long>(z) * npx;
     float lo = FLT_MAX, hi = -FLT_MAX;
     if ((npx & 3) == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
@@ -72,11 +76,14 @@ __global__ void __launch_bounds__(1024) k_slice_stats(const float* __restrict__ 
 // (CUDABackend.cu:46-50); imgT may then be null (the ray march reads rows). Both copies
 // use the zero-bordered layout of the projector (kFwdGuard pixels left and
 // right of every row, kFwdRows rows below the last); only the interior is
-// written here, the borders are zeroed when the buffers are set up.
+// written here, the borders are zeroed when the buffers are set up. With box
+// set, box[zg] = {x min, x max, y min, y max} of the pixels with a non-zero
+// value in any slice of the group (emptied by k_slice_stats): the projector
+// walks only that box, every pixel outside it being an exact zero.
 __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol, int w, int h, int nz,
                                                    const float4* __restrict__ stats,
                                                    float4* __restrict__ img, float4* __restrict__ imgT,
-                                                   int skip_zero) {
+                                                   int skip_zero, int4* __restrict__ box) {
     const long long pw = w + 2 * kFwdGuard, ph = h + 2 * kFwdGuard;  // row pitches
     const long long rw = h + kFwdRows, rh = w + kFwdRows;             // rows per plane
     __shared__ float4 tile[32][33];
@@ -93,6 +100,7 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
         lo[j] = st.x;
         inv[j] = __fdiv_rn(1.0f, st.z);
     }
+    int bx0 = INT_MAX, bx1 = -1, by0 = INT_MAX, by1 = -1;  // this thread's non-zero pixels
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int y = y0 + ty + 8 * r, x = x0 + tx;
@@ -106,10 +114,35 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
             }
         }
         const float4 q = make_float4(v[0], v[1], v[2], v[3]);
+        if (q.x != 0.0f || q.y != 0.0f || q.z != 0.0f || q.w != 0.0f) {
+            bx0 = min(bx0, x);
+            bx1 = max(bx1, x);
+            by0 = min(by0, y);
+            by1 = max(by1, y);
+        }
         tile[ty + 8 * r][tx] = q;
         if (x < w && y < h) img[(zg * rw + y) * pw + x + kFwdGuard] = q;
     }
+    __shared__ int4 wbox[8];  // per warp, then one set of atomics per block
+    if (box) {
+        bx0 = __reduce_min_sync(0xffffffffu, bx0);
+        bx1 = __reduce_max_sync(0xffffffffu, bx1);
+        by0 = __reduce_min_sync(0xffffffffu, by0);
+        by1 = __reduce_max_sync(0xffffffffu, by1);
+        if (tx == 0) wbox[ty] = make_int4(bx0, bx1, by0, by1);
+    }
     __syncthreads();
+    if (box && threadIdx.x == 0) {
+        int4 b = wbox[0];
+        for (int k = 1; k < 8; ++k)
+            b = make_int4(min(b.x, wbox[k].x), max(b.y, wbox[k].y), min(b.z, wbox[k].z), max(b.w, wbox[k].w));
+        if (b.y >= 0) {
+            atomicMin(&box[zg].x, b.x);
+            atomicMax(&box[zg].y, b.y);
+            atomicMin(&box[zg].z, b.z);
+            atomicMax(&box[zg].w, b.w);
+        }
+    }
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int x = x0 + ty + 8 * r, y = y0 + tx;
@@ -207,15 +240,16 @@ cudaError_t launch_trig(const float* d_angles_deg, int na, double2* d_cs, cudaSt
 }
 
 cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4* d_stats,
-                               cudaStream_t st) {
-    k_slice_stats<<<nz, 1024, 0, st>>>(d_vol, npx, d_stats);
+                               cudaStream_t st, int4* d_box) {
+    k_slice_stats<<<nz, 1024, 0, st>>>(d_vol, npx, d_stats, d_box);
     return cudaGetLastError();
 }
 
 cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
-                             float4* d_img, float4* d_imgT, cudaStream_t st, int skip_zero) {
+                             float4* d_img, float4* d_imgT, cudaStream_t st, int skip_zero,
+                             int4* d_box) {
     const dim3 grid((w + 31) / 32, (h + 31) / 32, (nz + 3) / 4);
-    k_normalize<<<grid, 256, 0, st>>>(d_vol, w, h, nz, d_stats, d_img, d_imgT, skip_zero);
+    k_normalize<<<grid, 256, 0, st>>>(d_vol, w, h, nz, d_stats, d_img, d_imgT, skip_zero, d_box);
     return cudaGetLastError();
 }
 

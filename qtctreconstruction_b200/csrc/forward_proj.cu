@@ -58,8 +58,9 @@ struct FAngle {
     float akq;     // |kq|: fraction per pixel step inside an interval
     float cf, sf;  // the reference's float cos/sin
     int a;
-    int p_lo, p_hi;
-    int edge;  // interval 0 or nd-1 of this CTA meets the image at this angle
+    int p_lo, p_hi;  // rows where an interval of the CTA meets the non-zero box
+    int c_lo, c_hi;  // columns of the non-zero box
+    int edge;        // interval 0 or nd-1 of this CTA meets the box at this angle
     int neg;   // kq < 0: crossings decrease with the bin
 };
 
@@ -80,19 +81,21 @@ __device__ __forceinline__ Bound boundary(const FAngle& f, int t, int p0) {
     return Bound{static_cast<int>(qfl), static_cast<float>(qstar - qfl)};
 }
 
-// A chunk is skipped exactly when both boundaries lie left of column -2, or
-// right of column nq + 1, at its first and last rows: the boundaries are
-// linear in the row, so the interval (at most sqrt 2 wide) then holds no image
-// pixel at any row of the chunk. Otherwise some boundary is within two columns
-// of the image at some row; moving at most one column per row, every
-// candidate column of the chunk stays within kFwdRows + 5 columns of the
-// image, inside the zero border (kFwdGuard = kFwdRows + 8).
-__device__ __forceinline__ bool chunk_meets_image(const Bound& ba, const Bound& bb, float dqf, int nq) {
+// A chunk is skipped exactly when both boundaries lie left of column
+// c_lo - 2, or right of column c_hi + 1, at its first and last rows, [c_lo,
+// c_hi] being the columns of the non-zero box (inside the image): the
+// boundaries are linear in the row, so the interval (at most sqrt 2 wide) then
+// holds only zero pixels at every row of the chunk. Otherwise some boundary is
+// within two columns of the image at some row; moving at most one column per
+// row, every candidate column of the chunk stays within kFwdRows + 5 columns
+// of the image, inside the zero border (kFwdGuard = kFwdRows + 8).
+__device__ __forceinline__ bool chunk_meets_box(const Bound& ba, const Bound& bb, float dqf, int c_lo,
+                                                int c_hi) {
     const float e = (PCH - 1) * dqf;
     const float a0 = static_cast<float>(ba.base) + ba.f, b0 = static_cast<float>(bb.base) + bb.f;
     const float lo = fminf(fminf(a0, a0 + e), fminf(b0, b0 + e));
     const float hi = fmaxf(fmaxf(a0, a0 + e), fmaxf(b0, b0 + e));
-    return hi >= -2.0f && lo <= static_cast<float>(nq + 1);
+    return hi >= static_cast<float>(c_lo - 2) && lo <= static_cast<float>(c_hi + 1);
 }
 
 __device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
@@ -200,6 +203,7 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
                                                         int h, int nz, int na, int nd, Trig trig,
                                                         const int4* __restrict__ groups,
                                                         const int* __restrict__ order,
+                                                        const int4* __restrict__ box,
                                                         float* __restrict__ sino) {
     __shared__ FAngle fa[GMAX];
 
@@ -221,21 +225,33 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
     const double dcf = static_cast<double>(nd / 2);
     constexpr double kReach = 2.0;  // an interval is at most sqrt 2 wide
 
-    // p range where crossings [qa, qb] (at p = 0) come within reach of the image
-    auto prange = [&](double qa, double qb, double dq, int& lo, int& hi) {
-        lo = 0;
-        hi = np - 1;
+    // p range (within rows [rl, rh]) where crossings [qa, qb] (at p = 0) come
+    // within reach of columns [cl, ch]
+    auto prange = [&](double qa, double qb, double dq, int cl, int ch, int rl, int rh, int& lo, int& hi) {
+        lo = rl;
+        hi = rh;
         if (dq != 0.0) {
-            const double pa0 = (-kReach - qa) / dq, pb0 = (nq - 1 + kReach - qa) / dq;
-            const double pa1 = (-kReach - qb) / dq, pb1 = (nq - 1 + kReach - qb) / dq;
-            lo = max(0, static_cast<int>(floor(fmin(fmin(pa0, pb0), fmin(pa1, pb1)))) - 1);
-            hi = min(np - 1, static_cast<int>(ceil(fmax(fmax(pa0, pb0), fmax(pa1, pb1)))) + 1);
-        } else if (fmax(qa, qb) < -kReach || fmin(qa, qb) > nq - 1 + kReach) {
+            const double pa0 = (cl - kReach - qa) / dq, pb0 = (ch + kReach - qa) / dq;
+            const double pa1 = (cl - kReach - qb) / dq, pb1 = (ch + kReach - qb) / dq;
+            lo = max(rl, static_cast<int>(floor(fmin(fmin(pa0, pb0), fmin(pa1, pb1)))) - 1);
+            hi = min(rh, static_cast<int>(ceil(fmax(fmax(pa0, pb0), fmax(pa1, pb1)))) + 1);
+        } else if (fmax(qa, qb) < cl - kReach || fmin(qa, qb) > ch + kReach) {
             hi = -1;
         }
     };
 
     if (tid < cnt) {
+        // the non-zero box of the CTA's slices (all its 4-slice groups), as
+        // walked rows [rl, rh] and gathered columns [cl, ch]
+        const int ng4 = (nz + 3) / 4;
+        int4 bx = box[blockIdx.z * NP];
+        for (int k = 1; k < NP; ++k) {
+            if (blockIdx.z * NP + k >= ng4) break;
+            const int4 b2 = box[blockIdx.z * NP + k];
+            bx = make_int4(min(bx.x, b2.x), max(bx.y, b2.y), min(bx.z, b2.z), max(bx.w, b2.w));
+        }
+        const int rl = rows ? bx.z : bx.x, rh = rows ? bx.w : bx.y;
+        const int cl = rows ? bx.x : bx.z, ch = rows ? bx.y : bx.w;
         const int a = order[grp.x + tid];
         const double2 tc = trig.cs[a];
         const double kq = rows ? tc.x : tc.y;
@@ -252,14 +268,20 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
         f.cf = tf.x;
         f.sf = tf.y;
         f.a = a;
-        prange(f.q0, f.q0 + tmax * f.inv, f.dq, f.p_lo, f.p_hi);
+        f.c_lo = cl;
+        f.c_hi = ch;
+        f.p_lo = 0;
+        f.p_hi = -1;
         f.edge = 0;
-        for (int ej : {0, nd - 1}) {
-            const int et = ej - jb;  // thread of the edge interval
-            if (et < 0 || et > nout) continue;
-            int lo, hi;
-            prange(f.q0 + et * f.inv, f.q0 + (et + 1) * f.inv, f.dq, lo, hi);
-            if (hi >= lo) f.edge = 1;
+        if (ch >= cl) {  // an empty box (all slices zero) leaves no rows
+            prange(f.q0, f.q0 + tmax * f.inv, f.dq, cl, ch, rl, rh, f.p_lo, f.p_hi);
+            for (int ej : {0, nd - 1}) {
+                const int et = ej - jb;  // thread of the edge interval
+                if (et < 0 || et > nout) continue;
+                int lo, hi;
+                prange(f.q0 + et * f.inv, f.q0 + (et + 1) * f.inv, f.dq, cl, ch, rl, rh, lo, hi);
+                if (hi >= lo) f.edge = 1;
+            }
         }
         fa[tid] = f;
     }
@@ -303,7 +325,7 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
         for (int p0 = wlo; p0 <= whi; p0 += PCH) {
             const Bound ba = boundary(f, tx, p0);
             const Bound bb = boundary(f, tx + 1, p0);
-            if (!chunk_meets_image(ba, bb, f.dqf, nq)) continue;
+            if (!chunk_meets_box(ba, bb, f.dqf, f.c_lo, f.c_hi)) continue;
             const float4* rowp = plane + static_cast<long long>(p0) * pitch;
             if (edge_a) acc = splat_rows_edge(rowp, pofs, pitch, f, ba, bb, p0, j, nd, rows, cxf, cyf, acc);
             else if (neg) splat_rows<-1>(rowp, pofs, pitch, ba, bb, f.dqf, acc.v, acc.d);
@@ -335,11 +357,12 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
 
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
                            int na, int nd, Trig trig, const int4* d_groups, int ngroups,
-                           const int* d_order, float* d_sino, unsigned* d_err, cudaStream_t st) {
+                           const int* d_order, const int4* d_box, float* d_sino, unsigned* d_err,
+                           cudaStream_t st) {
     (void)d_err;
     const dim3 grid((nd + OUT - 1) / OUT, ngroups, ((nz + 3) / 4 + NP - 1) / NP);
     k_forward<<<grid, dim3(FB, AY), 0, st>>>(d_img, d_imgT, w, h, nz, na, nd, trig, d_groups, d_order,
-                                             d_sino);
+                                             d_box, d_sino);
     return cudaGetLastError();
 }
 
