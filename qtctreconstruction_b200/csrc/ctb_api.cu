@@ -711,13 +711,46 @@ ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int dep
         num_angles > kMaxAngles)
         return fail(ctx, CTB_ERR_INVALID, "ctb_reconstruct_volume: invalid arguments");
     Guard g(ctx);
-    // Slabs of whole slice groups: the host->device copy of slab k + 1 and the
-    // device->host copy of slab k - 1 run on their own streams while slab k is
-    // reconstructed; slices are independent, so the result is the same as one
-    // pass over the volume. Two slab buffers each way.
+    // Slabs of whole 8-slice groups (the projector's groups, so the result is
+    // bit for bit that of one pass over the volume): the host->device copy of
+    // slab k + 1 and the device->host copy of slab k - 1 run on their own
+    // streams while slab k is reconstructed. Two slab buffers each way. The
+    // schedule tapers at both ends (a quarter slab, three quarters, full slabs,
+    // three quarters, a quarter), so the copy in before the first slab and the
+    // copy out after the last one, which nothing overlaps, are short.
     constexpr int kSlabs = 8;
-    const int slab = depth <= 16 ? depth : 4 * ((depth + 4 * kSlabs - 1) / (4 * kSlabs));
-    const int nslab = (depth + slab - 1) / slab;
+    std::vector<int2> slabs;  // {first slice, slices}
+    int slab = depth;
+    if (depth <= 16) {
+        slabs.push_back(make_int2(0, depth));
+    } else {
+        slab = 8 * ((depth + 8 * kSlabs - 1) / (8 * kSlabs));
+        const int rem = depth % 8;  // a partial last group goes at the very end
+        const int body = depth - rem;
+        const int q = slab >= 32 ? 8 * (slab / 32) : 0;  // a quarter slab, whole groups
+        std::vector<int> head, tail;
+        if (q > 0 && body >= 4 * slab) {
+            head = {q, slab - q};
+            tail = {slab - q, q};
+        }
+        int left = body;
+        for (int h : head) left -= h;
+        for (int h : tail) left -= h;
+        int z = 0;
+        for (int h : head) { slabs.push_back(make_int2(z, h)); z += h; }
+        while (left > 0) {
+            const int m = std::min(slab, left);
+            slabs.push_back(make_int2(z, m));
+            z += m;
+            left -= m;
+        }
+        for (int h : tail) { slabs.push_back(make_int2(z, h)); z += h; }
+        if (rem > 0) {
+            if (!slabs.empty() && slabs.back().y + rem <= slab) slabs.back().y += rem;
+            else slabs.push_back(make_int2(z, rem));
+        }
+    }
+    const int nslab = static_cast<int>(slabs.size());
     const size_t per = static_cast<size_t>(slab) * n * n;
     CTB_WS(ctx, d_in, float, "h_in", 2 * per);
     CTB_WS(ctx, d_out, float, "h_out", 2 * per);
@@ -744,7 +777,7 @@ ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int dep
     CTB_CUDA(ctx, cudaEventRecord(out_done[1], ctx->stream));
     for (int k = 0; k < nslab; ++k) {
         const int b = k & 1;
-        const int z0 = k * slab, nz = std::min(slab, depth - z0);
+        const int z0 = slabs[k].x, nz = slabs[k].y;
         const size_t off = static_cast<size_t>(z0) * n * n, cnt = static_cast<size_t>(nz) * n * n;
         float* in_b = d_in + b * per;
         float* out_b = d_out + b * per;

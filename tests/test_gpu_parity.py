@@ -275,12 +275,15 @@ def test_empty_inputs_return_empty(backend):
     assert r.size == 0
 
 
-def test_host_volume_pipeline_equals_device_path(backend):
-    """ctb_reconstruct_volume streams slabs (copies overlapped with compute);
-    the result must equal ctb_reconstruct_volume_d on the whole volume bit for bit."""
+@pytest.mark.parametrize("n,depth", [(96, 50), (40, 260)])
+def test_host_volume_pipeline_equals_device_path(backend, n, depth):
+    """ctb_reconstruct_volume streams slabs (copies overlapped with compute;
+    at depth 260 the schedule tapers at both ends and ends on a partial
+    8-slice group); the result must equal ctb_reconstruct_volume_d on the
+    whole volume bit for bit."""
     import torch
     rng = np.random.default_rng(17)
-    n, depth, na = 96, 50, 120
+    na = 120
     nd = ctb.odd_detector_count(n)
     vol = np.stack([ellipse_slice(rng, n, 3) for _ in range(depth)])
     host = backend.reconstructVolume(vol, ReconstructionParams(FilterType.SheppLogan, na), detector_bins=nd)
