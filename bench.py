@@ -66,7 +66,7 @@ def image_support(vol):
     the non-zero normalised pixels (raw != 0 and raw != the slice minimum;
     every other pixel contributes an exact zero, as the reference's skip of
     raw == 0 does), and the pixels of the per-8-slice-group bounding boxes of
-    those, which is what the projector walks."""
+    those, an upper bound of what the projector walks."""
     import numpy as np
     nz = vol.shape[0]
     lo = vol.reshape(nz, -1).min(axis=1)
@@ -408,9 +408,10 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
                     "algorithmic": "4 B (one float) per non-zero pixel-angle-slice: each non-zero pixel "
                                     "read once per angle",
                     "nonzero_fraction": nnz / (n * n * nz),
-                    "walked_fraction": walked / (n * n * nz),
-                    "note": "the projector walks, per 8-slice group, the bounding box of the non-zero "
-                            "normalised pixels; pixels outside it are exact zeros"}
+                    "box_fraction": walked / (n * n * nz),
+                    "note": "the projector walks, per 8-slice group, only where its intervals meet the "
+                            "bounding box and the centred disc of the non-zero normalised pixels (at most "
+                            "box_fraction of the pixels); the pixels outside are exact zeros"}
         roof_bp = {"kernel": "k_backproject", "bound": "smem", "achieved": achieved,
                    "peak": smem_gbs, "unit": "GB/s", "frac": achieved / smem_gbs,
                    "traffic": load_profile_traffic("backproject", args.config),

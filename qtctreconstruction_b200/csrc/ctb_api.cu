@@ -209,7 +209,7 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     const size_t elems = static_cast<size_t>(nzg) * std::max(fwd_plane_elems(h, w), fwd_plane_elems(w, h));
     CTB_WS(ctx, d_img, float4, "img", elems);
     CTB_WS(ctx, d_imgT, float4, "imgT", elems);
-    CTB_WS(ctx, d_box, int4, "fbox", nzg);
+    CTB_WS(ctx, d_box, int4, "fbox", 2 * nzg);  // per group: box, then disc
     // zero borders: cleared whenever the buffers or the plane geometry change
     const std::vector<long long> geom = {reinterpret_cast<long long>(d_img),
                                          reinterpret_cast<long long>(d_imgT), w, h, nzg};
@@ -715,9 +715,11 @@ ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int dep
     // bit for bit that of one pass over the volume): the host->device copy of
     // slab k + 1 and the device->host copy of slab k - 1 run on their own
     // streams while slab k is reconstructed. Two slab buffers each way. The
-    // schedule tapers at both ends (a quarter slab, three quarters, full slabs,
-    // three quarters, a quarter), so the copy in before the first slab and the
-    // copy out after the last one, which nothing overlaps, are short.
+    // schedule tapers at both ends (a quarter slab, three quarters, double
+    // slabs, three quarters, a quarter), so the copy in before the first slab
+    // and the copy out after the last one, which nothing overlaps, are short,
+    // while the middle launches are large enough to keep their tail waves
+    // small; each copy in stays shorter than the slab computed beside it.
     constexpr int kSlabs = 8;
     std::vector<int2> slabs;  // {first slice, slices}
     int slab = depth;
@@ -738,8 +740,9 @@ ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int dep
         for (int h : tail) left -= h;
         int z = 0;
         for (int h : head) { slabs.push_back(make_int2(z, h)); z += h; }
+        const int big = head.empty() ? slab : 2 * slab;
         while (left > 0) {
-            const int m = std::min(slab, left);
+            const int m = std::min(big, left);
             slabs.push_back(make_int2(z, m));
             z += m;
             left -= m;
@@ -751,6 +754,7 @@ ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int dep
         }
     }
     const int nslab = static_cast<int>(slabs.size());
+    for (const int2& sl : slabs) slab = std::max(slab, sl.y);
     const size_t per = static_cast<size_t>(slab) * n * n;
     CTB_WS(ctx, d_in, float, "h_in", 2 * per);
     CTB_WS(ctx, d_out, float, "h_out", 2 * per);

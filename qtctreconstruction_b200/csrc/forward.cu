@@ -28,7 +28,10 @@ __global__ void k_trig(const float* __restrict__ deg, int na, double2* __restric
 __global__ void __launch_bounds__(1024) k_slice_stats(const float* __restrict__ vol, long long npx,
                                                       float4* __restrict__ stats, int4* __restrict__ box) {
     const int z = blockIdx.x;
-    if (box && threadIdx.x == 0 && (z & 3) == 0) box[z >> 2] = make_int4(INT_MAX, -1, INT_MAX, -1);
+    if (box && threadIdx.x == 0 && (z & 3) == 0) {
+        box[2 * (z >> 2)] = make_int4(INT_MAX, -1, INT_MAX, -1);
+        box[2 * (z >> 2) + 1] = make_int4(-1, 0, 0, 0);
+    }
     const float* p = vol + static_cast<long long>(z) * npx;
     float lo = FLT_MAX, hi = -FLT_MAX;
     if ((npx & 3) == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
@@ -77,9 +80,12 @@ __global__ void __launch_bounds__(1024) k_slice_stats(const float* __restrict__ 
 // use the zero-bordered layout of the projector (kFwdGuard pixels left and
 // right of every row, kFwdRows rows below the last); only the interior is
 // written here, the borders are zeroed when the buffers are set up. With box
-// set, box[zg] = {x min, x max, y min, y max} of the pixels with a non-zero
-// value in any slice of the group (emptied by k_slice_stats): the projector
-// walks only that box, every pixel outside it being an exact zero.
+// set, box[2 zg] = {x min, x max, y min, y max} of the pixels with a non-zero
+// value in any slice of the group and box[2 zg + 1].x the largest
+// (2x - w + 1)^2 + (2y - h + 1)^2 among them (four times the squared distance
+// from the image centre; both emptied by k_slice_stats): the projector walks
+// only where its intervals meet that box and that disc, every other pixel
+// being an exact zero.
 __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol, int w, int h, int nz,
                                                    const float4* __restrict__ stats,
                                                    float4* __restrict__ img, float4* __restrict__ imgT,
@@ -101,6 +107,7 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
         inv[j] = __fdiv_rn(1.0f, st.z);
     }
     int bx0 = INT_MAX, bx1 = -1, by0 = INT_MAX, by1 = -1;  // this thread's non-zero pixels
+    int r4 = -1;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int y = y0 + ty + 8 * r, x = x0 + tx;
@@ -119,28 +126,39 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
             bx1 = max(bx1, x);
             by0 = min(by0, y);
             by1 = max(by1, y);
+            const int dx = 2 * x - w + 1, dy = 2 * y - h + 1;
+            r4 = max(r4, dx * dx + dy * dy);
         }
         tile[ty + 8 * r][tx] = q;
         if (x < w && y < h) img[(zg * rw + y) * pw + x + kFwdGuard] = q;
     }
     __shared__ int4 wbox[8];  // per warp, then one set of atomics per block
+    __shared__ int wr4[8];
     if (box) {
         bx0 = __reduce_min_sync(0xffffffffu, bx0);
         bx1 = __reduce_max_sync(0xffffffffu, bx1);
         by0 = __reduce_min_sync(0xffffffffu, by0);
         by1 = __reduce_max_sync(0xffffffffu, by1);
-        if (tx == 0) wbox[ty] = make_int4(bx0, bx1, by0, by1);
+        r4 = __reduce_max_sync(0xffffffffu, r4);
+        if (tx == 0) {
+            wbox[ty] = make_int4(bx0, bx1, by0, by1);
+            wr4[ty] = r4;
+        }
     }
     __syncthreads();
     if (box && threadIdx.x == 0) {
         int4 b = wbox[0];
-        for (int k = 1; k < 8; ++k)
+        int r = wr4[0];
+        for (int k = 1; k < 8; ++k) {
             b = make_int4(min(b.x, wbox[k].x), max(b.y, wbox[k].y), min(b.z, wbox[k].z), max(b.w, wbox[k].w));
+            r = max(r, wr4[k]);
+        }
         if (b.y >= 0) {
-            atomicMin(&box[zg].x, b.x);
-            atomicMax(&box[zg].y, b.y);
-            atomicMin(&box[zg].z, b.z);
-            atomicMax(&box[zg].w, b.w);
+            atomicMin(&box[2 * zg].x, b.x);
+            atomicMax(&box[2 * zg].y, b.y);
+            atomicMin(&box[2 * zg].z, b.z);
+            atomicMax(&box[2 * zg].w, b.w);
+            atomicMax(&box[2 * zg + 1].x, r);
         }
     }
 #pragma unroll

@@ -244,14 +244,17 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
         // the non-zero box of the CTA's slices (all its 4-slice groups), as
         // walked rows [rl, rh] and gathered columns [cl, ch]
         const int ng4 = (nz + 3) / 4;
-        int4 bx = box[blockIdx.z * NP];
+        int4 bx = box[2 * blockIdx.z * NP];
+        int r4 = box[2 * blockIdx.z * NP + 1].x;
         for (int k = 1; k < NP; ++k) {
             if (blockIdx.z * NP + k >= ng4) break;
-            const int4 b2 = box[blockIdx.z * NP + k];
+            const int4 b2 = box[2 * (blockIdx.z * NP + k)];
             bx = make_int4(min(bx.x, b2.x), max(bx.y, b2.y), min(bx.z, b2.z), max(bx.w, b2.w));
+            r4 = max(r4, box[2 * (blockIdx.z * NP + k) + 1].x);
         }
         const int rl = rows ? bx.z : bx.x, rh = rows ? bx.w : bx.y;
         const int cl = rows ? bx.x : bx.z, ch = rows ? bx.y : bx.w;
+        // every non-zero pixel lies within rad of the image centre
         const int a = order[grp.x + tid];
         const double2 tc = trig.cs[a];
         const double kq = rows ? tc.x : tc.y;
@@ -275,6 +278,26 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
         f.edge = 0;
         if (ch >= cl) {  // an empty box (all slices zero) leaves no rows
             prange(f.q0, f.q0 + tmax * f.inv, f.dq, cl, ch, rl, rh, f.p_lo, f.p_hi);
+            // Rows where the intervals' strip meets the disc: in the frame
+            // u' = (q - cq) kq + (p - cp) kp, v = (p - cp) kq - (q - cq) kp the
+            // strip is u' in [U0, U1] (boundaries t = 0 and tmax), the disc
+            // u'^2 + v^2 <= rad^2, and p - cp = u' kp + v kq. The rectangle
+            // u' in [max(U0, -rad), min(U1, rad)], |v| <= sqrt(rad^2 - m^2)
+            // (m the smallest |u'| there) holds their intersection.
+            const double rad = 0.5 * sqrt(static_cast<double>(r4)) + 1.5;
+            const double u0 = static_cast<double>(jb) - dcf, u1 = u0 + tmax;
+            const double a0 = fmax(fmin(u0, u1), -rad), a1 = fmin(fmax(u0, u1), rad);
+            if (a0 > a1) {
+                f.p_hi = -1;
+            } else {
+                const double m = (a0 <= 0.0 && a1 >= 0.0) ? 0.0 : fmin(fabs(a0), fabs(a1));
+                const double vm = sqrt(fmax(0.0, rad * rad - m * m));
+                const double e0 = a0 * kp, e1 = a1 * kp, ev = vm * fabs(kq);
+                const int dlo = static_cast<int>(floor(cp + fmin(e0, e1) - ev)) - 2;
+                const int dhi = static_cast<int>(ceil(cp + fmax(e0, e1) + ev)) + 2;
+                f.p_lo = max(f.p_lo, dlo);
+                f.p_hi = min(f.p_hi, dhi);
+            }
             for (int ej : {0, nd - 1}) {
                 const int et = ej - jb;  // thread of the edge interval
                 if (et < 0 || et > nout) continue;
