@@ -384,6 +384,17 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
     barrier()
     e2e_ms = e2.elapsed_time(e3) / e2e_steps
 
+    # ---- the forward projector walking the whole image (bounds off), for
+    # comparison with the bounded walk timed above; same results
+    be.set_forward_bounds(False)
+    step()
+    nb = 3
+    for _ in range(nb):
+        step()
+    torch.cuda.synchronize()
+    fwd_whole_ms = float(np.mean([be.stage_times(back)[1] for back in range(nb)]))
+    be.set_forward_bounds(True)
+
     ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms], "cuda")
 
     if rank == 0:
@@ -409,6 +420,7 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
                                     "read once per angle",
                     "nonzero_fraction": nnz / (n * n * nz),
                     "box_fraction": walked / (n * n * nz),
+                    "ms": fwd_ms, "ms_whole_image": fwd_whole_ms,
                     "note": "the projector walks, per 8-slice group, only where its intervals meet the "
                             "bounding box and the centred disc of the non-zero normalised pixels (at most "
                             "box_fraction of the pixels); the pixels outside are exact zeros"}

@@ -151,6 +151,14 @@ ctb_status ctb_autotune_load(ctb_ctx* ctx, const int* entries, int count);
 enum { CTB_CONVENTION_SERIAL = 0, CTB_CONVENTION_CUDA = 1 };
 ctb_status ctb_set_convention(ctb_ctx* ctx, int convention);
 
+/* Forward projector bounds (SerialBackend convention; on by default). The
+ * reference skips background pixels (SerialBackend.cpp:104-106). Here every
+ * pixel whose normalised value is zero is an exact zero contribution, so the
+ * projector walks each 8-slice group only where its detector intervals meet
+ * the bounding box and the centred disc of the group's non-zero pixels.
+ * enable = 0 walks the whole image (same results; for timing comparisons). */
+ctb_status ctb_set_forward_bounds(ctb_ctx* ctx, int enable);
+
 /* Measured shared-memory load bandwidth of this GPU in GB/s: a conflict-free
  * 16-byte-per-lane load loop over all SMs, timed with CUDA events. The
  * backprojector's roofline denominator. */

@@ -161,6 +161,7 @@ def _declare(L):
     L.ctb_extract_point_cloud.argtypes = [p, p, i, i, i, f, p, ctypes.c_int64, P(ctypes.c_int64)]
     L.ctb_set_profiling.argtypes = [p, i]
     L.ctb_set_filter_mode.argtypes = [p, i]
+    L.ctb_set_forward_bounds.argtypes = [p, i]
     L.ctb_set_bp_shape.argtypes = [p, i]
     L.ctb_bp_shape_info.argtypes = [i, P(i), P(i), P(i), P(i)]
     L.ctb_bp_shape_for.argtypes = [p, i, i, i, P(i)]
@@ -487,6 +488,13 @@ class B200Backend:
     def set_convention(self, convention: int):
         """CONVENTION_SERIAL (default, SerialBackend) or CONVENTION_CUDA (the reference CUDA backend)."""
         self._check(self._lib.ctb_set_convention(self._h, int(convention)), "set_convention")
+
+    def set_forward_bounds(self, enable: bool):
+        """Forward projector walks only the bounding box and centred disc of
+        each 8-slice group's non-zero pixels (default True; the other pixels
+        are exact zero contributions). False walks the whole image, with the
+        same results, for timing comparisons."""
+        self._check(self._lib.ctb_set_forward_bounds(self._h, 1 if enable else 0), "set_forward_bounds")
 
     def set_filter_mode(self, mode: int):
         """FILTER_MODE_FFT (default) or FILTER_MODE_TC_BF16X3 (tensor-core Toeplitz product)."""

@@ -220,8 +220,9 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     }
     Trig trig;
     CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
-    CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream,
-                                       ctx->convention == kConvCuda ? nullptr : d_box));
+    // the non-zero bounds (filled by normalisation) or, without them, none
+    int4* box = (ctx->convention == kConvCuda || !ctx->fwd_bounds) ? nullptr : d_box;
+    CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream, box));
     if (ctx->convention == kConvCuda) {
         CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, nullptr, ctx->stream, 0));
         mark(ctx, ev, 1);
@@ -229,13 +230,13 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
         CTB_LAUNCH(ctx, launch_raymarch(d_img, w, h, nz, na, nd, det_center, trig.cs, d_sino, ctx->stream));
         return CTB_OK;
     }
-    CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream, 1, d_box));
+    CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream, 1, box));
     mark(ctx, ev, 1);
     const ctb_ctx::FwdPlanDev* plan = nullptr;
     CTB_TRY(forward_plan_dev(ctx, angles_deg, na, w, h, nd, &plan));
     CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd, trig,
                                    static_cast<const int4*>(plan->groups.ptr), plan->ngroups,
-                                   static_cast<const int*>(plan->order.ptr), d_box, d_sino, ctx->d_err,
+                                   static_cast<const int*>(plan->order.ptr), box, d_sino, ctx->d_err,
                                    ctx->stream));
     return CTB_OK;
 }
@@ -509,6 +510,13 @@ ctb_status ctb_set_convention(ctb_ctx* ctx, int convention) {
     if (!ctx || (convention != CTB_CONVENTION_SERIAL && convention != CTB_CONVENTION_CUDA)) return CTB_ERR_INVALID;
     Guard g(ctx);
     ctx->convention = convention;
+    return CTB_OK;
+}
+
+ctb_status ctb_set_forward_bounds(ctb_ctx* ctx, int enable) {
+    if (!ctx || (enable != 0 && enable != 1)) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    ctx->fwd_bounds = enable;
     return CTB_OK;
 }
 

@@ -239,6 +239,7 @@ struct ctb_ctx {
     // Toeplitz tables per (bins, filter).
     int filter_mode = 0;
     int convention = 0;  // CTB_CONVENTION_SERIAL / CTB_CONVENTION_CUDA
+    int fwd_bounds = 1;  // forward projector walks only the non-zero bounds
     std::map<std::pair<int, int>, ctb::GemmTable> gemm_tables;
     // Backprojection tile shape: forced (>= 0), or per size bucket from the
     // autotuner, or bp_default_variant.

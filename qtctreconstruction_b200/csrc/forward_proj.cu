@@ -244,9 +244,10 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
         // the non-zero box of the CTA's slices (all its 4-slice groups), as
         // walked rows [rl, rh] and gathered columns [cl, ch]
         const int ng4 = (nz + 3) / 4;
-        int4 bx = box[2 * blockIdx.z * NP];
-        int r4 = box[2 * blockIdx.z * NP + 1].x;
-        for (int k = 1; k < NP; ++k) {
+        // without bounds: the whole image and a disc through its corners
+        int4 bx = box ? box[2 * blockIdx.z * NP] : make_int4(0, w - 1, 0, h - 1);
+        int r4 = box ? box[2 * blockIdx.z * NP + 1].x : (w - 1) * (w - 1) + (h - 1) * (h - 1);
+        for (int k = 1; k < NP && box; ++k) {
             if (blockIdx.z * NP + k >= ng4) break;
             const int4 b2 = box[2 * (blockIdx.z * NP + k)];
             bx = make_int4(min(bx.x, b2.x), max(bx.y, b2.y), min(bx.z, b2.z), max(bx.w, b2.w));
