@@ -422,8 +422,9 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
                     "box_fraction": walked / (n * n * nz),
                     "ms": fwd_ms, "ms_whole_image": fwd_whole_ms,
                     "note": "the projector walks, per 8-slice group, only where its intervals meet the "
-                            "bounding box and the centred disc of the non-zero normalised pixels (at most "
-                            "box_fraction of the pixels); the pixels outside are exact zeros"}
+                            "bounding box, the centred disc and the 8-row-band column ranges of the non-zero "
+                            "normalised pixels (at most box_fraction of the pixels); the pixels outside are "
+                            "exact zeros"}
         roof_bp = {"kernel": "k_backproject", "bound": "smem", "achieved": achieved,
                    "peak": smem_gbs, "unit": "GB/s", "frac": achieved / smem_gbs,
                    "traffic": load_profile_traffic("backproject", args.config),

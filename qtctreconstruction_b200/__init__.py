@@ -490,8 +490,9 @@ class B200Backend:
         self._check(self._lib.ctb_set_convention(self._h, int(convention)), "set_convention")
 
     def set_forward_bounds(self, enable: bool):
-        """Forward projector walks only the bounding box and centred disc of
-        each 8-slice group's non-zero pixels (default True; the other pixels
+        """Forward projector walks only the bounding box, centred disc and
+        8-row-band column ranges of each 8-slice group's non-zero pixels
+        (default True; the other pixels
         are exact zero contributions). False walks the whole image, with the
         same results, for timing comparisons."""
         self._check(self._lib.ctb_set_forward_bounds(self._h, 1 if enable else 0), "set_forward_bounds")

@@ -210,6 +210,8 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     CTB_WS(ctx, d_img, float4, "img", elems);
     CTB_WS(ctx, d_imgT, float4, "imgT", elems);
     CTB_WS(ctx, d_box, int4, "fbox", 2 * nzg);  // per group: box, then disc
+    const int nband = (h + 7) / 8 + (w + 7) / 8;  // per group: row bands, then column bands
+    CTB_WS(ctx, d_band, int2, "fband", static_cast<size_t>(nzg) * nband);
     // zero borders: cleared whenever the buffers or the plane geometry change
     const std::vector<long long> geom = {reinterpret_cast<long long>(d_img),
                                          reinterpret_cast<long long>(d_imgT), w, h, nzg};
@@ -222,7 +224,9 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
     // the non-zero bounds (filled by normalisation) or, without them, none
     int4* box = (ctx->convention == kConvCuda || !ctx->fwd_bounds) ? nullptr : d_box;
-    CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream, box));
+    int2* band = box ? d_band : nullptr;
+    CTB_LAUNCH(ctx, launch_slice_stats(d_vol, static_cast<long long>(w) * h, nz, d_stats, ctx->stream, box,
+                                       band, nband));
     if (ctx->convention == kConvCuda) {
         CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, nullptr, ctx->stream, 0));
         mark(ctx, ev, 1);
@@ -230,13 +234,13 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
         CTB_LAUNCH(ctx, launch_raymarch(d_img, w, h, nz, na, nd, det_center, trig.cs, d_sino, ctx->stream));
         return CTB_OK;
     }
-    CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream, 1, box));
+    CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream, 1, box, band));
     mark(ctx, ev, 1);
     const ctb_ctx::FwdPlanDev* plan = nullptr;
     CTB_TRY(forward_plan_dev(ctx, angles_deg, na, w, h, nd, &plan));
     CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd, trig,
                                    static_cast<const int4*>(plan->groups.ptr), plan->ngroups,
-                                   static_cast<const int*>(plan->order.ptr), box, d_sino, ctx->d_err,
+                                   static_cast<const int*>(plan->order.ptr), box, band, d_sino,
                                    ctx->stream));
     return CTB_OK;
 }

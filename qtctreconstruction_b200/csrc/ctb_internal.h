@@ -82,10 +82,11 @@ struct Trig {
 // of the launch.
 cudaError_t launch_trig(const float* d_angles_deg, int na, double2* d_cs, cudaStream_t st);
 cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4* d_stats,
-                               cudaStream_t st, int4* d_box = nullptr);
+                               cudaStream_t st, int4* d_box = nullptr, int2* d_band = nullptr,
+                               int nband = 0);
 cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
                              float4* d_img, float4* d_imgT, cudaStream_t st, int skip_zero = 1,
-                             int4* d_box = nullptr);
+                             int4* d_box = nullptr, int2* d_band = nullptr);
 // The reference CUDA backend's ray-march forward projector over the
 // normalised image planes (img only).
 cudaError_t launch_raymarch(const float4* d_img, int w, int h, int nz, int na, int nd, float det_center,
@@ -112,7 +113,7 @@ struct FwdPlan {
 FwdPlan forward_plan(const float* angles_deg, int na, int w, int h, int nd);
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
                            int na, int nd, Trig trig, const int4* d_groups, int ngroups,
-                           const int* d_order, const int4* d_box, float* d_sino, unsigned* d_err,
+                           const int* d_order, const int4* d_box, const int2* d_band, float* d_sino,
                            cudaStream_t st);
 cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
                           const FiltLayout& fl, const float2* d_Hc, const float2* d_tw,

@@ -26,12 +26,16 @@ __global__ void k_trig(const float* __restrict__ deg, int na, double2* __restric
 // With box set, also empties the non-zero bounding box of each 4-slice group
 // that k_normalize then fills.
 __global__ void __launch_bounds__(1024) k_slice_stats(const float* __restrict__ vol, long long npx,
-                                                      float4* __restrict__ stats, int4* __restrict__ box) {
+                                                      float4* __restrict__ stats, int4* __restrict__ box,
+                                                      int2* __restrict__ band, int nband) {
     const int z = blockIdx.x;
     if (box && threadIdx.x == 0 && (z & 3) == 0) {
         box[2 * (z >> 2)] = make_int4(INT_MAX, -1, INT_MAX, -1);
         box[2 * (z >> 2) + 1] = make_int4(-1, 0, 0, 0);
     }
+    if (band && (z & 3) == 0)
+        for (int i = threadIdx.x; i < nband; i += blockDim.x)
+            band[static_cast<long long>(z >> 2) * nband + i] = make_int2(INT_MAX, -1);
     const float* p = vol + static_cast<long long>(z) * npx;
     float lo = FLT_MAX, hi = -FLT_MAX;
     if ((npx & 3) == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
@@ -85,11 +89,14 @@ __global__ void __launch_bounds__(1024) k_slice_stats(const float* __restrict__ 
 // (2x - w + 1)^2 + (2y - h + 1)^2 among them (four times the squared distance
 // from the image centre; both emptied by k_slice_stats): the projector walks
 // only where its intervals meet that box and that disc, every other pixel
-// being an exact zero.
+// being an exact zero. With band set, the group's ceil(h/8) row bands (8 rows
+// each) get the x range of their non-zero pixels, followed by its ceil(w/8)
+// column bands with their y range (emptied by k_slice_stats too).
 __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol, int w, int h, int nz,
                                                    const float4* __restrict__ stats,
                                                    float4* __restrict__ img, float4* __restrict__ imgT,
-                                                   int skip_zero, int4* __restrict__ box) {
+                                                   int skip_zero, int4* __restrict__ box,
+                                                   int2* __restrict__ band) {
     const long long pw = w + 2 * kFwdGuard, ph = h + 2 * kFwdGuard;  // row pitches
     const long long rw = h + kFwdRows, rh = w + kFwdRows;             // rows per plane
     __shared__ float4 tile[32][33];
@@ -108,6 +115,7 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
     }
     int bx0 = INT_MAX, bx1 = -1, by0 = INT_MAX, by1 = -1;  // this thread's non-zero pixels
     int r4 = -1;
+    int rx[4];  // per row r: this thread's x if its pixel there is non-zero, else -1
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int y = y0 + ty + 8 * r, x = x0 + tx;
@@ -121,7 +129,9 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
             }
         }
         const float4 q = make_float4(v[0], v[1], v[2], v[3]);
-        if (q.x != 0.0f || q.y != 0.0f || q.z != 0.0f || q.w != 0.0f) {
+        const bool nzp = q.x != 0.0f || q.y != 0.0f || q.z != 0.0f || q.w != 0.0f;
+        rx[r] = nzp ? x : -1;
+        if (nzp) {
             bx0 = min(bx0, x);
             bx1 = max(bx1, x);
             by0 = min(by0, y);
@@ -134,6 +144,31 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
     }
     __shared__ int4 wbox[8];  // per warp, then one set of atomics per block
     __shared__ int wr4[8];
+    __shared__ int2 srow[4][8];  // [row band of the block][warp]: x range
+    __shared__ int2 scol[4][8];  // [column band of the block][warp]: y range
+    if (band) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int a = __reduce_min_sync(0xffffffffu, rx[r] >= 0 ? rx[r] : INT_MAX);
+            const int b = __reduce_max_sync(0xffffffffu, rx[r]);
+            if (tx == 0) srow[r][ty] = make_int2(a, b);
+        }
+        // this thread's column: y range of its non-zero pixels, reduced over
+        // the 8 lanes of its column band
+        int c0 = INT_MAX, c1 = -1;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (rx[r] >= 0) {
+                c0 = min(c0, y0 + ty + 8 * r);
+                c1 = max(c1, y0 + ty + 8 * r);
+            }
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            c0 = min(c0, __shfl_xor_sync(0xffffffffu, c0, o));
+            c1 = max(c1, __shfl_xor_sync(0xffffffffu, c1, o));
+        }
+        if ((tx & 7) == 0) scol[tx >> 3][ty] = make_int2(c0, c1);
+    }
     if (box) {
         bx0 = __reduce_min_sync(0xffffffffu, bx0);
         bx1 = __reduce_max_sync(0xffffffffu, bx1);
@@ -159,6 +194,23 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
             atomicMin(&box[2 * zg].z, b.z);
             atomicMax(&box[2 * zg].w, b.w);
             atomicMax(&box[2 * zg + 1].x, r);
+        }
+    }
+    if (band && threadIdx.x < 8) {
+        // threads 0..3: the block's row bands; 4..7: its column bands
+        const int k = threadIdx.x & 3;
+        const bool is_row = threadIdx.x < 4;
+        int2 b = is_row ? srow[k][0] : scol[k][0];
+        for (int t = 1; t < 8; ++t) {
+            const int2 c = is_row ? srow[k][t] : scol[k][t];
+            b = make_int2(min(b.x, c.x), max(b.y, c.y));
+        }
+        const int nby = (h + 7) / 8, nbx = (w + 7) / 8;
+        const int idx = is_row ? (y0 >> 3) + k : nby + (x0 >> 3) + k;
+        if (b.y >= 0 && idx < (is_row ? nby : nby + nbx)) {
+            int2* e = band + static_cast<long long>(zg) * (nby + nbx) + idx;
+            atomicMin(&e->x, b.x);
+            atomicMax(&e->y, b.y);
         }
     }
 #pragma unroll
@@ -258,16 +310,16 @@ cudaError_t launch_trig(const float* d_angles_deg, int na, double2* d_cs, cudaSt
 }
 
 cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4* d_stats,
-                               cudaStream_t st, int4* d_box) {
-    k_slice_stats<<<nz, 1024, 0, st>>>(d_vol, npx, d_stats, d_box);
+                               cudaStream_t st, int4* d_box, int2* d_band, int nband) {
+    k_slice_stats<<<nz, 1024, 0, st>>>(d_vol, npx, d_stats, d_box, d_band, nband);
     return cudaGetLastError();
 }
 
 cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
                              float4* d_img, float4* d_imgT, cudaStream_t st, int skip_zero,
-                             int4* d_box) {
+                             int4* d_box, int2* d_band) {
     const dim3 grid((w + 31) / 32, (h + 31) / 32, (nz + 3) / 4);
-    k_normalize<<<grid, 256, 0, st>>>(d_vol, w, h, nz, d_stats, d_img, d_imgT, skip_zero, d_box);
+    k_normalize<<<grid, 256, 0, st>>>(d_vol, w, h, nz, d_stats, d_img, d_imgT, skip_zero, d_box, d_band);
     return cudaGetLastError();
 }
 

@@ -32,6 +32,7 @@
 // lines. Warps never wait on one another, and the CTA's warps have nearly
 // equal row counts, so CTAs retire evenly. Accumulation runs on packed FP32x2
 // instructions.
+#include <climits>
 #include <cmath>
 
 #include "ctb_internal.h"
@@ -204,6 +205,7 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
                                                         const int4* __restrict__ groups,
                                                         const int* __restrict__ order,
                                                         const int4* __restrict__ box,
+                                                        const int2* __restrict__ band,
                                                         float* __restrict__ sino) {
     __shared__ FAngle fa[GMAX];
 
@@ -341,6 +343,11 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
     const bool neg = has_a && fa[ja].neg;
     const float cxf = static_cast<float>(w - 1) * 0.5f, cyf = static_cast<float>(h - 1) * 0.5f;
 
+    // 8-row bands of the walked axis: row bands (x ranges) of the group when
+    // walking rows, its column bands (y ranges) when walking columns
+    const int nby = (h + 7) / 8, nbx = (w + 7) / 8;
+    const int nb_all = nby + nbx, nb_off = rows ? 0 : nby, nb_p = rows ? nby : nbx;
+
     Sums acc;
 #pragma unroll
     for (int k = 0; k < 2 * NP; ++k) acc.v[k] = acc.d[k] = make_float2(0.f, 0.f);
@@ -349,7 +356,24 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
         for (int p0 = wlo; p0 <= whi; p0 += PCH) {
             const Bound ba = boundary(f, tx, p0);
             const Bound bb = boundary(f, tx + 1, p0);
-            if (!chunk_meets_box(ba, bb, f.dqf, f.c_lo, f.c_hi)) continue;
+            // the chunk's columns: the non-zero ranges of the 8-row bands its
+            // rows fall in, over the CTA's slice groups
+            int cl = f.c_lo, ch = f.c_hi;
+            if (band) {
+                cl = INT_MAX;
+                ch = -1;
+                const int b1 = min((p0 + PCH - 1) >> 3, nb_p - 1);
+                for (int k = 0; k < NP; ++k) {
+                    if (blockIdx.z * NP + k >= ng4) break;
+                    const int2* bk = band + static_cast<long long>(blockIdx.z * NP + k) * nb_all + nb_off;
+                    for (int bi = p0 >> 3; bi <= b1; ++bi) {
+                        const int2 r = __ldg(bk + bi);
+                        cl = min(cl, r.x);
+                        ch = max(ch, r.y);
+                    }
+                }
+            }
+            if (ch < cl || !chunk_meets_box(ba, bb, f.dqf, cl, ch)) continue;
             const float4* rowp = plane + static_cast<long long>(p0) * pitch;
             if (edge_a) acc = splat_rows_edge(rowp, pofs, pitch, f, ba, bb, p0, j, nd, rows, cxf, cyf, acc);
             else if (neg) splat_rows<-1>(rowp, pofs, pitch, ba, bb, f.dqf, acc.v, acc.d);
@@ -381,12 +405,11 @@ __global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict
 
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
                            int na, int nd, Trig trig, const int4* d_groups, int ngroups,
-                           const int* d_order, const int4* d_box, float* d_sino, unsigned* d_err,
+                           const int* d_order, const int4* d_box, const int2* d_band, float* d_sino,
                            cudaStream_t st) {
-    (void)d_err;
     const dim3 grid((nd + OUT - 1) / OUT, ngroups, ((nz + 3) / 4 + NP - 1) / NP);
     k_forward<<<grid, dim3(FB, AY), 0, st>>>(d_img, d_imgT, w, h, nz, na, nd, trig, d_groups, d_order,
-                                             d_box, d_sino);
+                                             d_box, d_band, d_sino);
     return cudaGetLastError();
 }
 
