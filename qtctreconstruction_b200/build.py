@@ -80,7 +80,8 @@ def build_cli(verbose: bool = False) -> str:
     os.makedirs(os.path.dirname(CLI), exist_ok=True)
     if os.path.exists(CLI) and os.path.getmtime(CLI) >= max(os.path.getmtime(CLI_SRC), os.path.getmtime(LIB)):
         return CLI
-    cmd = [NVCC, "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"), CLI_SRC, "-o", CLI,
+    cmd = [NVCC, "-std=c++17", "-O2", "-Wno-deprecated-gpu-targets", "-I" + os.path.join(ROOT, "include"),
+           CLI_SRC, "-o", CLI,
            "-L" + PKG, "-lctb200", "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/..", "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

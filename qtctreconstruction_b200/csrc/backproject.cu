@@ -311,15 +311,13 @@ __global__ void __launch_bounds__(THREADS, C::MINB) k_backproject(const __grid_c
         mbar_fence_init();
     }
     unsigned chunks = 0;
-    if (MODE == 0) {
+    if constexpr (MODE == 0) {
         __syncthreads();
         const BpJob& J = batch.job[0];
         const int zg = blockIdx.x / J.tiles;
         const int tl = blockIdx.x - zg * J.tiles;
         bp_tile<C>(S, J, zg, (tl % J.tiles_x) * C::TX, (tl / J.tiles_x) * C::TY, chunks, err);
-        return;
-    }
-    if (MODE == 1) {
+    } else if constexpr (MODE == 1) {
         __syncthreads();
         const int item = blockIdx.x;
         int j = 0;
@@ -329,21 +327,21 @@ __global__ void __launch_bounds__(THREADS, C::MINB) k_backproject(const __grid_c
         const int zg = local / J.tiles;
         const int tl = local - zg * J.tiles;
         bp_tile<C>(S, J, zg, (tl % J.tiles_x) * C::TX, (tl / J.tiles_x) * C::TY, chunks, err);
-        return;
-    }
-    for (;;) {
-        if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));
-        __syncthreads();
-        const int item = s_item;  // totals are below 2^31 (checked at launch)
-        if (item >= batch.total) break;
-        int j = 0;
-        while (j + 1 < batch.njobs && batch.job[j + 1].first <= item) ++j;
-        const BpJob& J = batch.job[j];
-        const int local = item - static_cast<int>(J.first);
-        const int zg = local / J.tiles;
-        const int tl = local - zg * J.tiles;
-        if (!bp_tile<C>(S, J, zg, (tl % J.tiles_x) * C::TX, (tl / J.tiles_x) * C::TY, chunks, err)) break;
-        __syncthreads();  // shared state of this item is dead before the next item's staging
+    } else {
+        for (;;) {
+            if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));
+            __syncthreads();
+            const int item = s_item;  // totals are below 2^31 (checked at launch)
+            if (item >= batch.total) break;
+            int j = 0;
+            while (j + 1 < batch.njobs && batch.job[j + 1].first <= item) ++j;
+            const BpJob& J = batch.job[j];
+            const int local = item - static_cast<int>(J.first);
+            const int zg = local / J.tiles;
+            const int tl = local - zg * J.tiles;
+            if (!bp_tile<C>(S, J, zg, (tl % J.tiles_x) * C::TX, (tl / J.tiles_x) * C::TY, chunks, err)) break;
+            __syncthreads();  // shared state of this item is dead before the next item's staging
+        }
     }
 }
 
