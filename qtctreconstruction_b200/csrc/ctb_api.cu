@@ -412,6 +412,7 @@ void ctb_destroy(ctb_ctx* ctx) {
         for (auto& e : ctx->slab_ev) cudaEventDestroy(e);
         if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
         if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
+        if (ctx->fbp_stream) cudaStreamDestroy(ctx->fbp_stream);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     }
     delete ctx;
@@ -768,55 +769,84 @@ ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int dep
     const int nslab = static_cast<int>(slabs.size());
     for (const int2& sl : slabs) slab = std::max(slab, sl.y);
     const size_t per = static_cast<size_t>(slab) * n * n;
+    const size_t per_sino = static_cast<size_t>(slab) * num_angles * detector_bins;
     CTB_WS(ctx, d_in, float, "h_in", 2 * per);
     CTB_WS(ctx, d_out, float, "h_out", 2 * per);
-    CTB_WS(ctx, d_sino, float, "sino", static_cast<size_t>(slab) * num_angles * detector_bins);
-    CTB_WS(ctx, d_stats, float4, "stats", slab);
+    CTB_WS(ctx, d_sino, float, "sino", 2 * per_sino);
+    CTB_WS(ctx, d_stats, float4, "stats", 2 * static_cast<size_t>(slab));
     if (!ctx->copy_in) {
         CTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
         CTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
     }
-    // events: per buffer {input landed, slab computed, output copied}; per slab {start, forward done, end}
-    const size_t need = 6 + 3 * static_cast<size_t>(nslab);
+    if (!ctx->fbp_stream) CTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->fbp_stream, cudaStreamNonBlocking));
+    // Two compute streams: the context's stream runs the forward stages, the
+    // FBP stream the filter and backprojection, so slab k's FBP overlaps slab
+    // k + 1's forward projection (each kernel's arithmetic is unchanged, so
+    // the result is still that of one pass). Buffers, two of each, pass
+    // between the streams by events: per buffer {input landed, forward done
+    // (input read, sinogram ready), FBP done (sinogram read, output ready),
+    // output copied}; per slab {start, forward done, end}.
+    const size_t need = 8 + 3 * static_cast<size_t>(nslab);
     while (ctx->slab_ev.size() < need) {
         cudaEvent_t e;
         CTB_CUDA(ctx, cudaEventCreate(&e));
         ctx->slab_ev.push_back(e);
     }
     cudaEvent_t* in_done = &ctx->slab_ev[0];
-    cudaEvent_t* computed = &ctx->slab_ev[2];
-    cudaEvent_t* out_done = &ctx->slab_ev[4];
-    cudaEvent_t* t = &ctx->slab_ev[6];
-    CTB_CUDA(ctx, cudaEventRecord(computed[0], ctx->stream));  // buffers start free
-    CTB_CUDA(ctx, cudaEventRecord(computed[1], ctx->stream));
-    CTB_CUDA(ctx, cudaEventRecord(out_done[0], ctx->stream));
-    CTB_CUDA(ctx, cudaEventRecord(out_done[1], ctx->stream));
+    cudaEvent_t* fwd_done = &ctx->slab_ev[2];
+    cudaEvent_t* fbp_done = &ctx->slab_ev[4];
+    cudaEvent_t* out_done = &ctx->slab_ev[6];
+    cudaEvent_t* t = &ctx->slab_ev[8];
+    cudaStream_t fwd_s = ctx->stream, fbp_s = ctx->fbp_stream;
+    for (int b = 0; b < 2; ++b) {  // buffers start free, after the caller's prior work
+        CTB_CUDA(ctx, cudaEventRecord(fwd_done[b], fwd_s));
+        CTB_CUDA(ctx, cudaEventRecord(fbp_done[b], fwd_s));
+        CTB_CUDA(ctx, cudaEventRecord(out_done[b], fwd_s));
+    }
+    // the FBP stages launch on ctx->stream: point it at the FBP stream for
+    // them and restore it on every exit
+    struct StreamSwap {
+        ctb_ctx* c;
+        cudaStream_t keep;
+        ~StreamSwap() { c->stream = keep; }
+    } swap{ctx, fwd_s};
     for (int k = 0; k < nslab; ++k) {
         const int b = k & 1;
         const int z0 = slabs[k].x, nz = slabs[k].y;
         const size_t off = static_cast<size_t>(z0) * n * n, cnt = static_cast<size_t>(nz) * n * n;
         float* in_b = d_in + b * per;
         float* out_b = d_out + b * per;
-        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_in, computed[b], 0));  // slab k - 2 no longer reads in_b
+        float* sino_b = d_sino + b * per_sino;
+        float4* stats_b = d_stats + b * static_cast<size_t>(slab);
+        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_in, fwd_done[b], 0));  // forward k - 2 read in_b
         CTB_CUDA(ctx, cudaMemcpyAsync(in_b, vol + off, cnt * sizeof(float), cudaMemcpyHostToDevice, ctx->copy_in));
         CTB_CUDA(ctx, cudaEventRecord(in_done[b], ctx->copy_in));
-        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, in_done[b], 0));
-        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, out_done[b], 0));  // slab k - 2 copied out of out_b
-        CTB_CUDA(ctx, cudaEventRecord(t[3 * k], ctx->stream));
-        CTB_TRY(forward_stage(ctx, in_b, n, n, nz, num_angles, detector_bins, nullptr, d_sino, d_stats, nullptr,
+        CTB_CUDA(ctx, cudaStreamWaitEvent(fwd_s, in_done[b], 0));
+        CTB_CUDA(ctx, cudaStreamWaitEvent(fwd_s, fbp_done[b], 0));  // FBP k - 2 read sino_b, stats_b
+        CTB_CUDA(ctx, cudaEventRecord(t[3 * k], fwd_s));
+        ctx->stream = fwd_s;
+        CTB_TRY(forward_stage(ctx, in_b, n, n, nz, num_angles, detector_bins, nullptr, sino_b, stats_b, nullptr,
                               true));
-        CTB_CUDA(ctx, cudaEventRecord(t[3 * k + 1], ctx->stream));
-        CTB_TRY(fbp_stage(ctx, d_sino, nz, num_angles, detector_bins, nullptr, n, filter, d_stats,
+        CTB_CUDA(ctx, cudaEventRecord(fwd_done[b], fwd_s));
+        CTB_CUDA(ctx, cudaEventRecord(t[3 * k + 1], fwd_s));
+        CTB_CUDA(ctx, cudaStreamWaitEvent(fbp_s, fwd_done[b], 0));
+        CTB_CUDA(ctx, cudaStreamWaitEvent(fbp_s, out_done[b], 0));  // slab k - 2 copied out of out_b
+        ctx->stream = fbp_s;
+        CTB_TRY(fbp_stage(ctx, sino_b, nz, num_angles, detector_bins, nullptr, n, filter, stats_b,
                           ctx->convention == kConvCuda ? CTB_DENORM_CUDA : CTB_DENORM_SERIAL, out_b, nullptr,
                           depth));
-        CTB_CUDA(ctx, cudaEventRecord(t[3 * k + 2], ctx->stream));
-        CTB_CUDA(ctx, cudaEventRecord(computed[b], ctx->stream));
-        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, computed[b], 0));
+        ctx->stream = fwd_s;
+        CTB_CUDA(ctx, cudaEventRecord(fbp_done[b], fbp_s));
+        CTB_CUDA(ctx, cudaEventRecord(t[3 * k + 2], fbp_s));
+        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, fbp_done[b], 0));
         CTB_CUDA(ctx, cudaMemcpyAsync(out + off, out_b, cnt * sizeof(float), cudaMemcpyDeviceToHost, ctx->copy_out));
         CTB_CUDA(ctx, cudaEventRecord(out_done[b], ctx->copy_out));
     }
     CTB_CUDA(ctx, cudaStreamSynchronize(ctx->copy_out));
-    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(fbp_s));
+    CTB_CUDA(ctx, cudaStreamSynchronize(fwd_s));
+    // stage sums (the stages of neighbouring slabs overlap, so these add up
+    // to more than the call's wall time)
     double fwd = 0.0, fbp = 0.0;
     for (int k = 0; k < nslab; ++k) {
         float a = 0.f, c = 0.f;

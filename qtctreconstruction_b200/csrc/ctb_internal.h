@@ -229,6 +229,7 @@ struct ctb_ctx {
     // Copy streams and per-slab events of the host-buffer volume pipeline
     // (created on first use).
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    cudaStream_t fbp_stream = nullptr;  // host volume path: slab k's FBP beside slab k+1's forward
     std::vector<cudaEvent_t> slab_ev;
 
     // Named workspaces, grown on demand and kept until destruction.
