@@ -19,8 +19,9 @@
 // launch filters any number of sinogram stacks that share Lc. The FFT is a
 // radix-16 Stockham transform (one
 // radix-2/4/8 pass when log2 L is not a multiple of 4) with twiddles read
-// from a double-precision-accurate table. Output rows are written as float4
-// (one value per slice), the layout the backprojector stages, scaled by
+// from a double-precision-accurate table. The last inverse pass writes its
+// natural-order samples straight to the output rows, float4 per bin (one
+// value per slice), the layout the backprojector stages, scaled by
 // pi/(2 na) times the slice's denormalisation span.
 #include <cmath>
 
@@ -188,6 +189,53 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int L, int Ns, int ti
     __syncthreads();
 }
 
+// Where the last inverse pass stores: sample e of the filtered row pair goes
+// to dst[2 (guard + e)] scaled by (s0, s1) when e < sq; the others are dropped.
+struct RowOut {
+    float2* dst;
+    int guard, sq;
+    float s0, s1;
+};
+
+// The last inverse pass (Ns = L / R): its Stockham output is in natural order,
+// sample j + r L/R in register r of butterfly j, so it is written straight to
+// the filtered row instead of back to shared memory (coalesced over j).
+template <int R, int K>
+__device__ __forceinline__ void last_pass_out(const float2* buf, int L, int tid, int T,
+                                              const float2* __restrict__ tw, const RowOut& o) {
+    constexpr int NB = 16 * K / R;
+    const int LR = L / R;  // = Ns
+    float2 v[NB][R];
+#pragma unroll
+    for (int bi = 0; bi < NB; ++bi) {
+        const int j = tid + bi * T;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[bi][r] = buf[padi(j + r * LR)];
+        if (LR > 1) {
+            const int step = 1;  // L / (Ns R)
+            if constexpr (R == 16) {
+                float2 w[16];
+                twiddles16<true>(tw, j * step, w);
+#pragma unroll
+                for (int r = 1; r < 16; ++r) v[bi][r] = cmul(v[bi][r], w[r]);
+            } else {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    float2 w = __ldg(tw + r * j * step);
+                    w.y = -w.y;
+                    v[bi][r] = cmul(v[bi][r], w);
+                }
+            }
+        }
+        dft<R, true>(v[bi]);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int e = j + r * LR;
+            if (e < o.sq) o.dst[2 * (o.guard + e)] = make_float2(v[bi][r].x * o.s0, v[bi][r].y * o.s1);
+        }
+    }
+}
+
 // First forward pass (Ns = 1): the inputs come straight from the two sinogram
 // rows (zero outside [pad, pad + nd)), so the zero-padded sequence is never
 // materialised.
@@ -260,7 +308,7 @@ __device__ __forceinline__ void fused_middle(float2* buf, int L, int tid, int T,
 template <int K>
 __device__ void filter_rows(float2* buf, int L, int logL, int tid, int T, const float* r0,
                             const float* r1, int pad, int nd, const float2* __restrict__ tw,
-                            const float2* __restrict__ Hc) {
+                            const float2* __restrict__ Hc, const RowOut& out) {
     const int rem = logL & 3;
     const int q = logL >> 2;  // radix-16 passes per transform (>= 1 for L >= 64)
     int Ns = 1;
@@ -275,13 +323,25 @@ __device__ void filter_rows(float2* buf, int L, int logL, int tid, int T, const 
     }
     fused_middle<K>(buf, L, tid, T, tw, Hc);
     Ns = 16;
-    for (int p = 0; p < q - 1; ++p) {
+    // the inverse radix-16 passes; the last pass of the transform stores the
+    // filtered rows itself
+    const int inv16 = q - 1 - (rem == 0 ? 1 : 0);
+    for (int p = 0; p < inv16; ++p) {
         stockham_pass<16, true, K>(buf, L, Ns, tid, T, tw);
         Ns *= 16;
     }
-    if (rem == 1) stockham_pass<2, true, K>(buf, L, Ns, tid, T, tw);
-    else if (rem == 2) stockham_pass<4, true, K>(buf, L, Ns, tid, T, tw);
-    else if (rem == 3) stockham_pass<8, true, K>(buf, L, Ns, tid, T, tw);
+    if (rem == 1) last_pass_out<2, K>(buf, L, tid, T, tw, out);
+    else if (rem == 2) last_pass_out<4, K>(buf, L, tid, T, tw, out);
+    else if (rem == 3) last_pass_out<8, K>(buf, L, tid, T, tw, out);
+    else if (q > 1) last_pass_out<16, K>(buf, L, tid, T, tw, out);
+    else {
+        // L = 16: the fused middle pass was the whole transform (natural order in buf)
+        for (int e = tid; e < L; e += T)
+            if (e < out.sq) {
+                const float2 u = buf[padi(e)];
+                out.dst[2 * (out.guard + e)] = make_float2(u.x * out.s0, u.y * out.s1);
+            }
+    }
 }
 
 // Per-slice output scale: pi/(2 na) times the denormalisation span.
@@ -298,9 +358,11 @@ __device__ __forceinline__ float slice_scale(const float4* stats, int z, int nz,
 
 // One CTA per item (slice pair zp, angle a) of a job of the batch; block
 // T = Lc/(16 K) threads filter slices 2 zp and 2 zp + 1 at angle a; dynamic smem
-// (Lc + Lc/16) float2. An item's arithmetic depends only on its own job.
+// (Lc + Lc/16) float2. An item's arithmetic depends only on its own job. With
+// K = 1 the registers are held to 80 (three 256-thread or six 128-thread CTAs
+// per SM), which measured faster than the compiler's own allocation.
 template <int K>
-__global__ void __launch_bounds__(256) k_filter(const __grid_constant__ FiltBatch batch, int logL) {
+__global__ void __launch_bounds__(256, (K == 1 ? 3 : 1)) k_filter(const __grid_constant__ FiltBatch batch, int logL) {
     extern __shared__ float2 smem[];
     const long long item = blockIdx.x + static_cast<long long>(blockIdx.y) * gridDim.x;
     if (item >= batch.total) return;
@@ -315,22 +377,18 @@ __global__ void __launch_bounds__(256) k_filter(const __grid_constant__ FiltBatc
     const int tid = threadIdx.x;
     const float* r0 = J.sino + (static_cast<long long>(z0) * na + a) * nd;
     const float* r1 = z1 < nz ? J.sino + (static_cast<long long>(z1) * na + a) * nd : nullptr;
-    filter_rows<K>(smem, batch.Lc, logL, tid, T, r0, r1, J.pad, nd, batch.tw, J.Hc);
-    const float s0 = slice_scale(J.stats, z0, nz, J.denorm, J.scale);
-    const float s1 = slice_scale(J.stats, z1, nz, J.denorm, J.scale);
     // rows z0, z1 are lanes (z0 % 4, z0 % 4 + 1) of the float4 layout
     const int pitch = J.pitch, guard = J.guard, sq = J.sq;
     float2* dst = reinterpret_cast<float2*>(J.filt + (static_cast<long long>(z0 / 4) * na + a) * pitch) +
                   ((z0 & 3) >> 1);
-    for (int i = tid; i < pitch; i += T) {
-        const int j = i - guard;
-        float2 o = make_float2(0.f, 0.f);
-        if (j >= 0 && j < sq) {
-            const float2 u = smem[padi(j)];
-            o = make_float2(u.x * s0, u.y * s1);
-        }
-        dst[2 * i] = o;
+    const RowOut out{dst, guard, sq, slice_scale(J.stats, z0, nz, J.denorm, J.scale),
+                     slice_scale(J.stats, z1, nz, J.denorm, J.scale)};
+    // guard bins on both sides of the row are zeros
+    for (int i = tid; i < pitch - sq; i += T) {
+        const int b = i < guard ? i : i + sq;
+        dst[2 * b] = make_float2(0.f, 0.f);
     }
+    filter_rows<K>(smem, batch.Lc, logL, tid, T, r0, r1, J.pad, nd, batch.tw, J.Hc, out);
 }
 
 }  // namespace
