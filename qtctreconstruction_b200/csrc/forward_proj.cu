@@ -199,7 +199,7 @@ __device__ __noinline__ Sums splat_rows_edge(const float4* __restrict__ rowp, lo
     return acc;
 }
 
-__global__ void __launch_bounds__(THREADS, 6) k_forward(const float4* __restrict__ img,
+__global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict__ img,
                                                         const float4* __restrict__ imgT, int w,
                                                         int h, int nz, int na, int nd, Trig trig,
                                                         const int4* __restrict__ groups,
