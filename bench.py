@@ -97,6 +97,55 @@ def circle_voxels(n: int) -> int:
     return c
 
 
+# ---------------------------------------------------------------- accuracy
+ACC_GATE = {"rel_l2": 1e-5, "max_abs": 1e-4}
+
+
+def accuracy_slices(nz: int, n: int):
+    """Slices whose output is checked: both sides of the 8-slice group and
+    slab boundaries of the host pipeline's schedule, the middle and the ends
+    (fewer at n >= 1024, where one FP64 slice takes seconds)."""
+    if n >= 1024:
+        zs = [0, 15, 16, nz // 2 - 1, nz // 2, nz - 1]
+    else:
+        zs = [0, 15, 16, 63, 64, nz // 2 - 1, nz // 2, nz - 65, nz - 64, nz - 1]
+    return sorted({z for z in zs if 0 <= z < nz})
+
+
+def accuracy_report(vol_host, outputs: dict, na: int, nd: int, kind: int, zs):
+    """Error of each reconstructed volume in `outputs` (name -> (nz, n, n)
+    array) on the slices `zs` against the FP64 rerun of SerialBackend's
+    reconstructVolume (oracle, per slice: slices are independent), and against
+    SerialBackend's own float path (reported, not gated: at n = 512 the float
+    reference itself is ~3e-5 from FP64). Worst slice of each. The oracle
+    calls run in threads (they release the GIL)."""
+    import concurrent.futures as cf
+
+    import numpy as np
+
+    import oracle as O
+
+    def one(z, f64):
+        v = np.ascontiguousarray(vol_host[z:z + 1])
+        return (O.reconstruct_volume_f64 if f64 else O.reconstruct_volume_f32)(v, na, nd, kind)[0]
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(2 * len(zs), os.cpu_count() or 1))) as ex:
+        f64 = dict(zip(zs, ex.map(lambda z: one(z, True), zs)))
+        f32 = dict(zip(zs, ex.map(lambda z: one(z, False), zs)))
+    rep = {"slices": list(zs), "gate_vs_fp64": ACC_GATE,
+           "reference": "FP64 rerun of SerialBackend::reconstructVolume (oracle); serial = its float path",
+           "serial_vs_fp64": {"rel_l2": max(O.rel_l2(f32[z], f64[z]) for z in zs),
+                              "max_abs": max(O.max_abs_rel(f32[z], f64[z]) for z in zs)}}
+    for name, out in outputs.items():
+        r = {"rel_l2_vs_fp64": max(O.rel_l2(out[z], f64[z]) for z in zs),
+             "max_abs_vs_fp64": max(O.max_abs_rel(out[z], f64[z]) for z in zs),
+             "rel_l2_vs_serial": max(O.rel_l2(out[z], f32[z]) for z in zs),
+             "max_abs_vs_serial": max(O.max_abs_rel(out[z], f32[z]) for z in zs)}
+        r["pass"] = r["rel_l2_vs_fp64"] <= ACC_GATE["rel_l2"] and r["max_abs_vs_fp64"] <= ACC_GATE["max_abs"]
+        rep[name] = r
+    return rep
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
@@ -213,10 +262,11 @@ def replica_throughput(world: int, units_per_rank: float, ms: float) -> float:
 
 
 # ------------------------------------------------------------- CPU baseline
-def cpu_reference_rate(cfg: dict, slices: int, params, repeats: int = 1):
+def cpu_reference_rate(cfg: dict, slices: int, params, repeats: int = 3):
     """The reference's OpenMPBackend per-slice path (computeSinogram with the
-    config's odd detector + reconstructSlice) on `slices` slices of the
-    phantom, all host threads. Returns (updates/s, threads, kind, isa)."""
+    config's odd detector + reconstructSlice) on `slices` central slices of the
+    phantom, all host threads, after one warm-up slice; the median of
+    `repeats` timed runs. Returns (updates/s, threads, kind, isa, sample)."""
     import numpy as np
 
     import oracle as O
@@ -239,23 +289,23 @@ def cpu_reference_rate(cfg: dict, slices: int, params, repeats: int = 1):
     # warm-up on one slice
     s, a, mm = R.compute_sinogram(R.OPENMP, vol[0], na, nd, lib=lib)
     R.reconstruct_slice(R.OPENMP, s, a, n, kind, mm[0], mm[1], lib=lib)
-    best = None
+    times = []
     for _ in range(repeats):
         t0 = time.perf_counter()
         for z in range(slices):
             s, a, mm = R.compute_sinogram(R.OPENMP, vol[z], na, nd, lib=lib)
             R.reconstruct_slice(R.OPENMP, s, a, n, kind, mm[0], mm[1], lib=lib)
-        dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
-    sample = f"{slices} of {nz} slices, OpenMPBackend computeSinogram(nd={nd}) + reconstructSlice, {isa}"
-    return n * n * slices * na / best, threads, "reference", isa, sample
+        times.append(time.perf_counter() - t0)
+    sample = (f"{slices} central of {nz} slices, OpenMPBackend computeSinogram(nd={nd}) + reconstructSlice, "
+              f"{isa}, median of {repeats} runs")
+    return n * n * slices * na / statistics.median(times), threads, "reference", isa, sample
 
 
-def cpu_native_rate(cfg: dict, slices: int, params):
+def cpu_native_rate(cfg: dict, slices: int, params, repeats: int = 3):
     """The reference OpenMPBackend's own reconstructVolume (its native volume
     path: detector bins = N, symmetric-z SIMD backprojection) on `slices`
-    slices of the phantom, all host threads. Returns (updates/s, threads) or
-    None when the reference build is absent."""
+    slices of the phantom, all host threads; the median of `repeats` runs.
+    Returns (updates/s, threads) or None when the reference build is absent."""
     import oracle as O
     from oracle import reference as R
     lib, _ = R.timing_lib()
@@ -266,18 +316,20 @@ def cpu_native_rate(cfg: dict, slices: int, params):
     threads = os.cpu_count() or 1
     lib.ref_set_threads(threads)
     R.reconstruct_volume(R.OPENMP, vol[:2], na, kind, lib=lib)  # warm-up
-    t0 = time.perf_counter()
-    R.reconstruct_volume(R.OPENMP, vol, na, kind, lib=lib)
-    dt = time.perf_counter() - t0
-    return n * n * slices * na / dt, threads
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        R.reconstruct_volume(R.OPENMP, vol, na, kind, lib=lib)
+        times.append(time.perf_counter() - t0)
+    return n * n * slices * na / statistics.median(times), threads
 
 
 def run_reference(args, cfg, rank: int, world: int):
     """--impl reference: the reference's CPU path, rank 0 only."""
     if rank != 0:
         return 0
-    import qtctreconstruction_b200 as ctb  # host-side parameter generation only (no GPU)
-    params = ctb.phantom_params(cfg["seed"], cfg["ellipsoids"])
+    import oracle as O  # the phantom's seeded parameter draw; the product library is never loaded
+    params = O.phantom_params(cfg["seed"], cfg["ellipsoids"])
     n, nz, na = cfg["n"], cfg["nz"], cfg["na"]
     slices = args.ref_slices
     for _ in range(args.warmup if args.warmup < 2 else 1):
@@ -285,8 +337,9 @@ def run_reference(args, cfg, rank: int, world: int):
     rates = []
     threads, kind, isa, sample = 1, "port", "", ""
     for _ in range(args.steps):
-        r, threads, kind, isa, sample = cpu_reference_rate(cfg, slices, params)
+        r, threads, kind, isa, sample = cpu_reference_rate(cfg, slices, params, repeats=1)
         rates.append(r)
+    sample = sample.replace("median of 1 runs", f"median over {args.steps} steps")
     value = statistics.median(rates)
     step_ms = n * n * slices * na / value * 1e3
     line = {
@@ -398,6 +451,12 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
     ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms], "cuda")
 
     if rank == 0:
+        # accuracy of the timed outputs themselves: the device-resident step's
+        # volume and the end-to-end call's host volume
+        acc = None
+        if not args.no_accuracy:
+            acc = accuracy_report(hin.numpy(), {"device": out.cpu().numpy(), "e2e": hout.numpy()}, na, nd, kind,
+                                  accuracy_slices(nz, n))
         value = replica_throughput(world, updates, ms)
         smem_gbs = be.probe_smem_bandwidth()
         inside = circle_voxels(n) * nz * na
@@ -458,18 +517,24 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
                     "ms_per_step": e2e_ms, "api": "ctb_reconstruct_volume (pinned host buffers)"},
             "clocks": clocks,
         }
+        if acc is not None:
+            for k in ("rel_l2_vs_fp64", "max_abs_vs_fp64", "rel_l2_vs_serial"):
+                line[k] = acc["device"][k]
+            line["e2e"].update({k: acc["e2e"][k] for k in ("rel_l2_vs_fp64", "max_abs_vs_fp64", "rel_l2_vs_serial")})
+            line["accuracy"] = acc
         if args.filter_modes:
             line["filter_modes"] = filter_mode_report(args, cfg, be, stream, vol, out, params, peaks)
         if world == 1 and not args.no_cpu_baseline:
             r, threads, kind_b, isa, sample = cpu_reference_rate(cfg, args.ref_slices, params)
             line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": threads, "kind": kind_b,
                                     "sample": sample}
-            nat = cpu_native_rate(cfg, 4 * args.ref_slices, params)
+            nat = cpu_native_rate(cfg, 2 * args.ref_slices, params)
             if nat:
                 line["cpu_baseline_native"] = {
                     "value": nat[0], "unit": UNIT, "cores": nat[1], "kind": "reference",
-                    "sample": f"{4 * args.ref_slices} of {cfg['nz']} slices, OpenMPBackend::reconstructVolume "
-                              "(its native volume path, detector bins = N)"}
+                    "sample": f"{2 * args.ref_slices} central of {cfg['nz']} slices, "
+                              "OpenMPBackend::reconstructVolume (its native volume path, detector bins = N), "
+                              "median of 3 runs"}
         print(json.dumps(line), flush=True)
     be.close()
     if dist is not None:
@@ -786,8 +851,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="large")
-    ap.add_argument("--ref-slices", type=int, default=2, help="slices per CPU baseline sample")
+    ap.add_argument("--ref-slices", type=int, default=16, help="central slices per CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the check of the timed outputs against the FP64 oracle")
     ap.add_argument("--filter-modes", action="store_true",
                     help="also time the tensor-core filter and compare both filters with FP64 (default for precision)")
     args = ap.parse_args()

@@ -165,6 +165,22 @@ ctb_status ctb_set_forward_bounds(ctb_ctx* ctx, int enable);
  * backprojector's roofline denominator. */
 ctb_status ctb_probe_smem_bandwidth(ctb_ctx* ctx, double* gbs);
 
+/* Diagnostics. The reference reports device failures by printing or throwing
+ * (CUDABackend.cu:37-43, HybridBackend.cu:44-65); here every device-side wait
+ * is bounded and a wait that gives up makes the call return CTB_ERR_TIMEOUT
+ * with the context still usable.
+ * ctb_selftest_bounded_wait runs that path on purpose: one CTA waits, at most
+ * `polls` polls per thread, on a barrier that nothing completes (no copy is
+ * in flight), records the timeout and returns. It returns CTB_ERR_TIMEOUT
+ * when the path works (and CTB_OK would mean the wait was not bounded).
+ * ctb_set_fault_injection (host side, for tests): with slab >= 0 the next
+ * ctb_reconstruct_volume calls fail with CTB_ERR_CUDA after queuing that
+ * slab's copy and forward stage, with earlier slabs still in flight; such a
+ * failed call returns only after all its copies and kernels have finished.
+ * -1 (the default) turns it off. */
+ctb_status ctb_selftest_bounded_wait(ctb_ctx* ctx, unsigned polls);
+ctb_status ctb_set_fault_injection(ctb_ctx* ctx, int slab);
+
 /* Geometry helpers shared with the reference (SerialBackend.cpp:152-163):
  * square_bins = ceil(sqrt(2)*bins), pad_before = square_bins/2 - bins/2,
  * fft_size = max(64, nextPow2(2*square_bins)). */
@@ -233,14 +249,16 @@ ctb_status ctb_fbp_d(ctb_ctx* ctx, const float* d_sino, int depth, int num_angle
                      const float* angles_deg, int output_size, int filter, const float* d_stats,
                      int denorm, float* d_out);
 
-/* Ramp filtering + backprojection of 1..4 slices that allocates no device
+/* Filtering (any CTB_FILTER_* id; others return CTB_ERR_INVALID) +
+ * backprojection of 1..4 slices that allocates no device
  * memory; it has no counterpart in the reference. It exists for callers that
  * cannot allocate device memory where they reconstruct (a caller-owned memory
  * pool, a real-time loop that must not wait on an allocator, a host whose
  * allocator is not cudaMalloc) and so cannot create a context, whose
  * workspaces are allocated on demand. The caller passes device buffers
  * d_sino[depth][num_angles][bins] and d_out[depth][output_size]^2; the result
- * is in normalised units, as ctb_fbp_d with d_stats = NULL, and the call
+ * is in normalised units (no denormalisation: the same values as ctb_fbp_d
+ * with d_stats = NULL and as SerialBackend::reconstructSlice), and the call
  * returns after `stream` (a cudaStream_t, NULL = legacy default stream) has
  * finished it. Every intermediate lives in one static 16 MiB device array that
  * each GPU using the library keeps until the process exits: at most 2048

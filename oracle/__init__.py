@@ -78,6 +78,7 @@ def _declare_oracle(L):
     L.orc_backproject_f64.argtypes = [_F64P, i, i, _F32P, i, _F64P]
     L.orc_reconstruct_volume_f32.argtypes = [_F32P, i, i, i, i, i, _F32P]
     L.orc_reconstruct_volume_f64.argtypes = [_F32P, i, i, i, i, i, _F64P]
+    L.orc_phantom_params.argtypes = [ctypes.c_uint64, i, _F32P]
     L.orc_phantom_sum.argtypes = [_F32P, i, i, i, i, _F32P]
     L.orc_phantom_sum_slab.argtypes = [_F32P, i, i, i, i, i, i, _F32P]
     L.orc_generator3d.argtypes = [i, i, i, f, i, ctypes.c_uint, _F32P, _F32P]
@@ -211,6 +212,13 @@ def reconstruct_volume_f64(vol: np.ndarray, na: int, nd: int, kind: int) -> np.n
 
 
 # ----------------------------------------------------------------- phantoms
+def phantom_params(seed: int, count: int) -> np.ndarray:
+    """Ellipsoid records (count, 16) float32 of the seeded benchmark phantom."""
+    p = np.zeros(max(count, 1) * 16, np.float32)
+    _ok(lib().orc_phantom_params(seed, count, p), "phantom_params")
+    return p[: count * 16].reshape(count, 16)
+
+
 def phantom_sum(params: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
     p = np.ascontiguousarray(params, np.float32).reshape(-1)
     k = p.size // 16

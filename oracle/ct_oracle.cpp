@@ -636,6 +636,48 @@ int orc_reconstruct_volume_f64(const float* vol, int n, int nz, int na, int nd, 
 // Phantoms
 // ---------------------------------------------------------------------------
 
+// Ellipsoid records of the benchmark phantom, drawn from a seeded 64-bit
+// Mersenne twister in this order per ellipsoid: centre ~ U[-0.6, 0.6]^3,
+// semi-axes ~ U[0.05, 0.4]^3, a rotation as a normalised quaternion of four
+// standard normals (redrawn while its squared norm is below 1e-12), density
+// ~ U[-0.3, 1.0]. The draw order and distributions define the phantom, so they
+// are fixed; the timed CPU baseline draws its phantom here and never loads the
+// product library.
+int orc_phantom_params(uint64_t seed, int count, float* out) {
+    if (count < 0 || (count > 0 && !out)) return 1;
+    std::mt19937_64 gen(seed);
+    std::uniform_real_distribution<double> centre(-0.6, 0.6), semi(0.05, 0.4), density(-0.3, 1.0);
+    std::normal_distribution<double> normal(0.0, 1.0);
+    for (int e = 0; e < count; ++e) {
+        double c[3], s[3], q[4];
+        for (double& v : c) v = centre(gen);
+        for (double& v : s) v = semi(gen);
+        double norm2;
+        do {
+            norm2 = 0.0;
+            for (double& v : q) {
+                v = normal(gen);
+                norm2 += v * v;
+            }
+        } while (norm2 < 1e-12);
+        const double len = std::sqrt(norm2);
+        const double w = q[0] / len, a = q[1] / len, b = q[2] / len, d = q[3] / len;
+        const double rho = density(gen);
+        float* r = out + 16 * e;
+        r[0] = static_cast<float>(c[0]);
+        r[1] = static_cast<float>(c[1]);
+        r[2] = static_cast<float>(c[2]);
+        // rows of the world -> body rotation of the unit quaternion (w, a, b, d)
+        const double m[9] = {1 - 2 * (b * b + d * d), 2 * (a * b + w * d),     2 * (a * d - w * b),
+                             2 * (a * b - w * d),     1 - 2 * (a * a + d * d), 2 * (b * d + w * a),
+                             2 * (a * d + w * b),     2 * (b * d - w * a),     1 - 2 * (a * a + b * b)};
+        for (int i = 0; i < 9; ++i) r[3 + i] = static_cast<float>(m[i]);
+        for (int i = 0; i < 3; ++i) r[12 + i] = static_cast<float>(1.0 / (s[i] * s[i]));
+        r[15] = static_cast<float>(rho);
+    }
+    return 0;
+}
+
 // Summed random-ellipsoid phantom (the benchmark phantom). params holds k
 // records of 16 floats: centre (3), rotation rows R (9, body = R * (p - c)),
 // inverse squared semi-axes (3), density (1). Voxel coordinates are

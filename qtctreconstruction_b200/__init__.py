@@ -103,6 +103,8 @@ class ServerStats(ctypes.Structure):
                [("memory_budget", ctypes.c_size_t), ("memory_peak", ctypes.c_size_t)]
 
 
+STATUS_OK, STATUS_INVALID, STATUS_CUDA, STATUS_OOM, STATUS_UNSUPPORTED = 0, 1, 2, 3, 4  # ctb_status
+STATUS_NO_DEVICE, STATUS_TIMEOUT, STATUS_CANCELLED, STATUS_NOT_FOUND, STATUS_BUSY = 5, 6, 7, 8, 9
 REQ_DEVICE = 1     # CTB_REQ_DEVICE
 CONVENTION_SERIAL = 0       # CTB_CONVENTION_SERIAL
 CONVENTION_CUDA = 1         # CTB_CONVENTION_CUDA
@@ -174,6 +176,8 @@ def _declare(L):
     L.ctb_filter_kernel_ms.argtypes = [p, i, P(ctypes.c_double)]
     L.ctb_stage_times.argtypes = [p, i, P(ctypes.c_double)]
     L.ctb_probe_smem_bandwidth.argtypes = [p, P(ctypes.c_double)]
+    L.ctb_selftest_bounded_wait.argtypes = [p, ctypes.c_uint]
+    L.ctb_set_fault_injection.argtypes = [p, i]
     L.ctb_batch_create.argtypes = [p, P(FbpJob), i, i, P(p)]
     L.ctb_batch_run.argtypes = [p]
     L.ctb_batch_info.argtypes = [p, P(i), P(ctypes.c_double), P(ctypes.c_size_t)]
@@ -546,6 +550,15 @@ class B200Backend:
         g = ctypes.c_double()
         self._check(self._lib.ctb_probe_smem_bandwidth(self._h, ctypes.byref(g)), "probe_smem_bandwidth")
         return g.value
+
+    def selftest_bounded_wait(self, polls: int) -> int:
+        """Run the device timeout path on purpose (ctb_selftest_bounded_wait);
+        returns the raw status, STATUS_TIMEOUT when the wait gave up as it should."""
+        return int(self._lib.ctb_selftest_bounded_wait(self._h, int(polls)))
+
+    def set_fault_injection(self, slab: int):
+        """Test hook: ctb_reconstruct_volume fails after queuing slab `slab` (-1 = off)."""
+        self._check(self._lib.ctb_set_fault_injection(self._h, int(slab)), "set_fault_injection")
 
     def reconstruct_volume_d(self, d_vol: int, n: int, depth: int, na: int, nd: int, kind: int, d_out: int):
         self._check(self._lib.ctb_reconstruct_volume_d(self._h, ctypes.c_void_p(d_vol), n, depth, na, nd,

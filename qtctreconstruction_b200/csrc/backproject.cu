@@ -88,14 +88,33 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
         "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
     return ok != 0;
 }
-// Bounded wait: gives up after 2^22 polls (each poll itself suspends for a
-// hardware-defined interval) and reports through the device error word.
+// Bounded wait: gives up after `polls` polls (2^22 in the kernels; each poll
+// itself suspends for a hardware-defined interval) and reports `code` through
+// the device error word.
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
-                                                  unsigned* err) {
-    for (unsigned it = 0; it < (1u << 22); ++it)
+                                                  unsigned* err, unsigned polls = 1u << 22,
+                                                  unsigned code = 1u) {
+    for (unsigned it = 0; it < polls; ++it)
         if (mbar_try_wait(bar, parity)) return true;
-    if (err) atomicOr(err, 1u);
+    if (err) atomicOr(err, code);
     return false;
+}
+
+// Self-test of the timeout path: one CTA initialises an mbarrier that expects
+// one arrival which never comes (no copy or thread arrives on it), and every
+// thread waits on it through the same bounded wait the kernels use. Each wait
+// gives up after `polls` polls and records kWaitSelftestCode; the kernel then
+// returns normally. Nothing is in flight when it exits.
+constexpr unsigned kWaitSelftestCode = 1u << 4;
+__global__ void k_wait_selftest(unsigned polls, unsigned* err) {
+    __shared__ unsigned long long bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    mbar_wait_bounded(&bar, 0, err, polls, kWaitSelftestCode);
+    __syncthreads();
 }
 
 struct AngleRec {
@@ -389,6 +408,11 @@ BpShape shape_of() {
 }
 
 }  // namespace
+
+cudaError_t launch_wait_selftest(unsigned polls, unsigned* d_err, cudaStream_t st) {
+    k_wait_selftest<<<1, 64, 0, st>>>(polls, d_err);
+    return cudaGetLastError();
+}
 
 BpShape bp_shape(int variant) {
     switch (variant) {

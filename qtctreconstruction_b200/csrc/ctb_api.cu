@@ -212,12 +212,17 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     CTB_WS(ctx, d_box, int4, "fbox", 2 * nzg);  // per group: box, then disc
     const int nband = (h + 7) / 8 + (w + 7) / 8;  // per group: row bands, then column bands
     CTB_WS(ctx, d_band, int2, "fband", static_cast<size_t>(nzg) * nband);
-    // zero borders: cleared whenever the buffers or the plane geometry change
+    // zero borders: the planes of every group sit at fixed offsets for a
+    // given (w, h), and normalisation writes only their interiors, so the
+    // buffers' whole capacity is cleared once whenever the buffers or the plane
+    // geometry change; any later group count up to the capacity reuses it
+    const size_t cap = std::min(ctx->ws["img"].bytes, ctx->ws["imgT"].bytes) / sizeof(float4);
     const std::vector<long long> geom = {reinterpret_cast<long long>(d_img),
-                                         reinterpret_cast<long long>(d_imgT), w, h, nzg};
+                                         reinterpret_cast<long long>(d_imgT), w, h,
+                                         static_cast<long long>(cap)};
     if (ctx->img_border_geom != geom) {
-        CTB_CUDA(ctx, cudaMemsetAsync(d_img, 0, sizeof(float4) * elems, ctx->stream));
-        CTB_CUDA(ctx, cudaMemsetAsync(d_imgT, 0, sizeof(float4) * elems, ctx->stream));
+        CTB_CUDA(ctx, cudaMemsetAsync(d_img, 0, sizeof(float4) * cap, ctx->stream));
+        CTB_CUDA(ctx, cudaMemsetAsync(d_imgT, 0, sizeof(float4) * cap, ctx->stream));
         ctx->img_border_geom = geom;
     }
     Trig trig;
@@ -242,6 +247,29 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
                                    static_cast<const int4*>(plan->groups.ptr), plan->ngroups,
                                    static_cast<const int*>(plan->order.ptr), box, band, d_sino,
                                    ctx->stream));
+    return CTB_OK;
+}
+
+// Grow every workspace forward_stage and fbp_stage use for a volume of
+// nz_max slices of n x n (nd bins, n x n output) to its final size, so that a
+// pipeline of smaller slabs never reallocates (cudaFree synchronises the whole
+// device) between its launches.
+ctb_status reserve_volume_workspaces(ctb_ctx* ctx, int n, int nz_max, int na, int nd) {
+    const int nzg = (nz_max + 3) / 4;
+    const size_t elems = static_cast<size_t>(nzg) * fwd_plane_elems(n, n);
+    const int nband = 2 * ((n + 7) / 8);
+    CTB_WS(ctx, d_img, float4, "img", elems);
+    CTB_WS(ctx, d_imgT, float4, "imgT", elems);
+    CTB_WS(ctx, d_box, int4, "fbox", 2 * nzg);
+    CTB_WS(ctx, d_band, int2, "fband", static_cast<size_t>(nzg) * nband);
+    const PadGeom g = pad_geometry(nd);
+    const FiltLayout fl = filt_layout(g.sq, n);
+    CTB_WS(ctx, d_filt, float4, "filt", static_cast<size_t>(nzg) * na * fl.pitch);
+    if (ctx->filter_mode == CTB_FILTER_MODE_TC_BF16X3) {
+        CTB_WS(ctx, d_split, unsigned char, "gemm_split", filter_gemm_split_bytes(nz_max, na, nd));
+        (void)d_split;
+    }
+    (void)d_img; (void)d_imgT; (void)d_box; (void)d_band; (void)d_filt;
     return CTB_OK;
 }
 
@@ -573,6 +601,21 @@ ctb_status ctb_filter_kernel_ms(ctb_ctx* ctx, int back, double* ms) {
     return CTB_OK;
 }
 
+ctb_status ctb_selftest_bounded_wait(ctb_ctx* ctx, unsigned polls) {
+    if (!ctx || polls == 0) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    CTB_TRY(check_error_word(ctx));  // a stale error word is not this test's
+    CTB_LAUNCH(ctx, launch_wait_selftest(polls, ctx->d_err, ctx->stream));
+    return check_error_word(ctx);
+}
+
+ctb_status ctb_set_fault_injection(ctb_ctx* ctx, int slab) {
+    if (!ctx || slab < -1) return CTB_ERR_INVALID;
+    Guard g(ctx);
+    ctx->fault_slab = slab;
+    return CTB_OK;
+}
+
 ctb_status ctb_probe_smem_bandwidth(ctb_ctx* ctx, double* gbs) {
     if (!ctx || !gbs) return CTB_ERR_INVALID;
     Guard g(ctx);
@@ -774,6 +817,7 @@ ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int dep
     CTB_WS(ctx, d_out, float, "h_out", 2 * per);
     CTB_WS(ctx, d_sino, float, "sino", 2 * per_sino);
     CTB_WS(ctx, d_stats, float4, "stats", 2 * static_cast<size_t>(slab));
+    CTB_TRY(reserve_volume_workspaces(ctx, n, slab, num_angles, detector_bins));
     if (!ctx->copy_in) {
         CTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
         CTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
@@ -803,13 +847,25 @@ ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int dep
         CTB_CUDA(ctx, cudaEventRecord(fbp_done[b], fwd_s));
         CTB_CUDA(ctx, cudaEventRecord(out_done[b], fwd_s));
     }
-    // the FBP stages launch on ctx->stream: point it at the FBP stream for
-    // them and restore it on every exit
-    struct StreamSwap {
+    // The FBP stages launch on ctx->stream: it points at the FBP stream for
+    // them and is restored on every exit. An exit before the loop completes
+    // (a failed launch, copy or workspace) first drains all four streams, so
+    // that no queued copy still reads `vol` or writes `out`, and no kernel
+    // still uses the slab buffers, once the call has returned.
+    struct PipelineExit {
         ctb_ctx* c;
         cudaStream_t keep;
-        ~StreamSwap() { c->stream = keep; }
-    } swap{ctx, fwd_s};
+        bool finished = false;
+        ~PipelineExit() {
+            if (!finished) {
+                cudaStreamSynchronize(c->copy_in);
+                cudaStreamSynchronize(keep);
+                cudaStreamSynchronize(c->fbp_stream);
+                cudaStreamSynchronize(c->copy_out);
+            }
+            c->stream = keep;
+        }
+    } pipeline_exit{ctx, fwd_s};
     for (int k = 0; k < nslab; ++k) {
         const int b = k & 1;
         const int z0 = slabs[k].x, nz = slabs[k].y;
@@ -828,6 +884,8 @@ ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int dep
         CTB_TRY(forward_stage(ctx, in_b, n, n, nz, num_angles, detector_bins, nullptr, sino_b, stats_b, nullptr,
                               true));
         CTB_CUDA(ctx, cudaEventRecord(fwd_done[b], fwd_s));
+        if (k == ctx->fault_slab)  // test hook: fail with this slab's copy and forward stage queued
+            return fail(ctx, CTB_ERR_CUDA, "injected fault after queuing slab %d of %d", k, nslab);
         CTB_CUDA(ctx, cudaEventRecord(t[3 * k + 1], fwd_s));
         CTB_CUDA(ctx, cudaStreamWaitEvent(fbp_s, fwd_done[b], 0));
         CTB_CUDA(ctx, cudaStreamWaitEvent(fbp_s, out_done[b], 0));  // slab k - 2 copied out of out_b
@@ -845,6 +903,8 @@ ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int dep
     CTB_CUDA(ctx, cudaStreamSynchronize(ctx->copy_out));
     CTB_CUDA(ctx, cudaStreamSynchronize(fbp_s));
     CTB_CUDA(ctx, cudaStreamSynchronize(fwd_s));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->copy_in));
+    pipeline_exit.finished = true;
     // stage sums (the stages of neighbouring slabs overlap, so these add up
     // to more than the call's wall time)
     double fwd = 0.0, fbp = 0.0;

@@ -203,6 +203,10 @@ cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltL
                                int n_out, Trig trig, const float4* d_stats, int denorm,
                                float* d_out, unsigned* d_err, cudaStream_t st, int variant = 0,
                                int convention = kConvSerial);
+// One CTA whose threads wait, at most `polls` polls each, on an mbarrier that
+// nothing completes; each records a timeout in *d_err (the timeout path's
+// self-test).
+cudaError_t launch_wait_selftest(unsigned polls, unsigned* d_err, cudaStream_t st);
 cudaError_t launch_point_count(const float* d_vol, long long total, float thr,
                                unsigned* d_block_counts, int blocks, cudaStream_t st);
 cudaError_t launch_point_write(const float* d_vol, int nx, int ny, long long total, float thr,
@@ -261,6 +265,7 @@ struct ctb_ctx {
     std::map<std::vector<long long>, FwdPlanDev> fwd_plans;
     std::vector<long long> img_border_geom;  // geometry the image borders were zeroed for
     unsigned* d_err = nullptr;  // device error word for bounded waits
+    int fault_slab = -1;        // host-side fault injection in the volume pipeline (tests)
 
     // Stage profiling: a ring of event sets, one set per volume reconstruction.
     static constexpr int kProfRing = 256;

@@ -72,7 +72,8 @@ extern "C" ctb_status ctb_fbp_noalloc(const float* d_sino, int depth, int num_an
                                       const float* angles_deg, int output_size, int filter,
                                       float* d_out, void* stream) {
     using namespace ctb;
-    if (!d_sino || !d_out || depth <= 0 || num_angles <= 0 || bins <= 0 || output_size <= 0)
+    if (!d_sino || !d_out || depth <= 0 || num_angles <= 0 || bins <= 0 || output_size <= 0 ||
+        filter < CTB_FILTER_RAMP || filter > CTB_FILTER_BARTLETT)
         return CTB_ERR_INVALID;
     const PadGeom g = pad_geometry(bins);
     const FiltLayout fl = filt_layout(g.sq, output_size);
@@ -135,6 +136,8 @@ extern "C" ctb_status ctb_fbp_noalloc(const float* d_sino, int depth, int num_an
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d_err, sizeof h_err, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamSynchronize(st);  // nothing queued may outlive the host tables above
         cudaGetLastError();
         return CTB_ERR_CUDA;
     }

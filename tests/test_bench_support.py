@@ -52,3 +52,35 @@ def test_image_support_random_against_direct_count():
         if z % 4 == 0:
             v[z] = np.where(v[z] == 0, v[z].min(), v[z])  # background at the minimum
     assert bench.image_support(v) == _direct(v)
+
+
+def test_oracle_phantom_params_equal_library_bit_for_bit():
+    """The timed CPU baseline draws the benchmark phantom from the oracle's
+    restatement of the seeded parameter draw, so that it never loads the
+    product library; both must give the same records bit for bit."""
+    import oracle as O
+    import qtctreconstruction_b200 as ctb
+    for seed, count in [(1, 10), (2, 32), (3, 64), (4, 24), (5, 1), (2**40 + 17, 9), (7, 0)]:
+        a = O.phantom_params(seed, count)
+        b = ctb.phantom_params(seed, count)
+        assert a.shape == b.shape == (count, 16)
+        np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_reference_arm_loads_no_product_library():
+    """bench.py --impl reference runs the reference's CPU path only: after it,
+    no shared object of the product package is mapped into the process."""
+    import subprocess
+    code = ("import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--config', 'small', "
+            "'--steps', '1', '--warmup', '0', '--ref-slices', '1']; "
+            "import bench; bench.main(); "
+            "maps = open('/proc/self/maps').read(); "
+            "assert 'libctb200' not in maps, 'product library loaded'; "
+            "assert 'qtctreconstruction_b200' not in sys.modules, 'product package imported'")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
+    import json
+    d = json.loads(line)
+    assert d["impl"] == "reference" and d["value"] > 0
