@@ -167,18 +167,19 @@ ctb_status ctb_probe_smem_bandwidth(ctb_ctx* ctx, double* gbs);
 
 /* Diagnostics. The reference reports device failures by printing or throwing
  * (CUDABackend.cu:37-43, HybridBackend.cu:44-65); here every device-side wait
- * is bounded and a wait that gives up makes the call return CTB_ERR_TIMEOUT
- * with the context still usable.
+ * is bounded (2 s of the GPU's global timer) and a wait that gives up makes
+ * the call return CTB_ERR_TIMEOUT with the context still usable.
  * ctb_selftest_bounded_wait runs that path on purpose: one CTA waits, at most
- * `polls` polls per thread, on a barrier that nothing completes (no copy is
- * in flight), records the timeout and returns. It returns CTB_ERR_TIMEOUT
- * when the path works (and CTB_OK would mean the wait was not bounded).
+ * `limit_us` microseconds (1 .. 2e6), on a barrier that nothing completes (no
+ * copy is in flight), records the timeout and returns. It returns
+ * CTB_ERR_TIMEOUT when the path works (CTB_OK would mean the wait was not
+ * bounded).
  * ctb_set_fault_injection (host side, for tests): with slab >= 0 the next
  * ctb_reconstruct_volume calls fail with CTB_ERR_CUDA after queuing that
  * slab's copy and forward stage, with earlier slabs still in flight; such a
  * failed call returns only after all its copies and kernels have finished.
  * -1 (the default) turns it off. */
-ctb_status ctb_selftest_bounded_wait(ctb_ctx* ctx, unsigned polls);
+ctb_status ctb_selftest_bounded_wait(ctb_ctx* ctx, unsigned limit_us);
 ctb_status ctb_set_fault_injection(ctb_ctx* ctx, int slab);
 
 /* Geometry helpers shared with the reference (SerialBackend.cpp:152-163):

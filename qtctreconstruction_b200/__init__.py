@@ -551,10 +551,11 @@ class B200Backend:
         self._check(self._lib.ctb_probe_smem_bandwidth(self._h, ctypes.byref(g)), "probe_smem_bandwidth")
         return g.value
 
-    def selftest_bounded_wait(self, polls: int) -> int:
-        """Run the device timeout path on purpose (ctb_selftest_bounded_wait);
-        returns the raw status, STATUS_TIMEOUT when the wait gave up as it should."""
-        return int(self._lib.ctb_selftest_bounded_wait(self._h, int(polls)))
+    def selftest_bounded_wait(self, limit_us: int) -> int:
+        """Run the device timeout path on purpose (ctb_selftest_bounded_wait):
+        a wait of at most limit_us microseconds on a barrier nothing completes.
+        Returns the raw status, STATUS_TIMEOUT when the wait gave up as it should."""
+        return int(self._lib.ctb_selftest_bounded_wait(self._h, int(limit_us)))
 
     def set_fault_injection(self, slab: int):
         """Test hook: ctb_reconstruct_volume fails after queuing slab `slab` (-1 = off)."""

@@ -88,14 +88,25 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
         "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
     return ok != 0;
 }
-// Bounded wait: gives up after `polls` polls (2^22 in the kernels; each poll
-// itself suspends for a hardware-defined interval) and reports `code` through
-// the device error word.
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait: gives up once `limit_ns` nanoseconds of the GPU's global timer
+// have passed since the first unsuccessful poll (2 s in the kernels; a poll may
+// itself suspend for a hardware-defined interval, so the bound is on time, with
+// 2^22 polls as a second cap), and reports `code` through the device error word.
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
-                                                  unsigned* err, unsigned polls = 1u << 22,
+                                                  unsigned* err,
+                                                  unsigned long long limit_ns = 2000000000ull,
                                                   unsigned code = 1u) {
-    for (unsigned it = 0; it < polls; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (unsigned it = 0; it < (1u << 22); ++it) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > limit_ns) break;
+    }
     if (err) atomicOr(err, code);
     return false;
 }
@@ -103,17 +114,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
 // Self-test of the timeout path: one CTA initialises an mbarrier that expects
 // one arrival which never comes (no copy or thread arrives on it), and every
 // thread waits on it through the same bounded wait the kernels use. Each wait
-// gives up after `polls` polls and records kWaitSelftestCode; the kernel then
-// returns normally. Nothing is in flight when it exits.
+// gives up after `limit_us` microseconds and records kWaitSelftestCode; the
+// kernel then returns normally. Nothing is in flight when it exits.
 constexpr unsigned kWaitSelftestCode = 1u << 4;
-__global__ void k_wait_selftest(unsigned polls, unsigned* err) {
+__global__ void k_wait_selftest(unsigned limit_us, unsigned* err) {
     __shared__ unsigned long long bar;
     if (threadIdx.x == 0) {
         mbar_init(&bar, 1);
         mbar_fence_init();
     }
     __syncthreads();
-    mbar_wait_bounded(&bar, 0, err, polls, kWaitSelftestCode);
+    mbar_wait_bounded(&bar, 0, err, 1000ull * limit_us, kWaitSelftestCode);
     __syncthreads();
 }
 
@@ -409,8 +420,8 @@ BpShape shape_of() {
 
 }  // namespace
 
-cudaError_t launch_wait_selftest(unsigned polls, unsigned* d_err, cudaStream_t st) {
-    k_wait_selftest<<<1, 64, 0, st>>>(polls, d_err);
+cudaError_t launch_wait_selftest(unsigned limit_us, unsigned* d_err, cudaStream_t st) {
+    k_wait_selftest<<<1, 64, 0, st>>>(limit_us, d_err);
     return cudaGetLastError();
 }
 

@@ -101,7 +101,7 @@ ctb_status trig_table(ctb_ctx* ctx, const float* angles_deg, int na, Trig* out) 
 }
 
 // Convolution spectrum (conv_response) per (fft size, filter, bins), and the
-// twiddle table exp(-2 pi i k / Lc) per convolution length.
+// FFT twiddle tables (fft_twiddle_table) per convolution length.
 ctb_status filter_tables(ctb_ctx* ctx, const PadGeom& g, int type, const float2** d_Hc,
                          const float2** d_tw, bool keep_nyquist) {
     const int Lc = g.Lc;
@@ -120,14 +120,10 @@ ctb_status filter_tables(ctb_ctx* ctx, const PadGeom& g, int type, const float2*
     }
     auto jt = ctx->twiddles.find(Lc);
     if (jt == ctx->twiddles.end()) {
-        std::vector<float2> tw(Lc);
-        for (int i = 0; i < Lc; ++i) {
-            const double ang = 2.0 * 3.14159265358979323846 * static_cast<double>(i) / Lc;
-            tw[i] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(-std::sin(ang)));
-        }
+        const std::vector<float2> tw = fft_twiddle_table(Lc);
         DevBuf b;
-        CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float2) * Lc));
-        b.bytes = sizeof(float2) * Lc;
+        CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float2) * tw.size()));
+        b.bytes = sizeof(float2) * tw.size();
         CTB_CUDA(ctx, cudaMemcpy(b.ptr, tw.data(), b.bytes, cudaMemcpyHostToDevice));
         jt = ctx->twiddles.emplace(Lc, b).first;
     }
@@ -601,11 +597,11 @@ ctb_status ctb_filter_kernel_ms(ctb_ctx* ctx, int back, double* ms) {
     return CTB_OK;
 }
 
-ctb_status ctb_selftest_bounded_wait(ctb_ctx* ctx, unsigned polls) {
-    if (!ctx || polls == 0) return CTB_ERR_INVALID;
+ctb_status ctb_selftest_bounded_wait(ctb_ctx* ctx, unsigned limit_us) {
+    if (!ctx || limit_us == 0 || limit_us > 2000000u) return CTB_ERR_INVALID;
     Guard g(ctx);
     CTB_TRY(check_error_word(ctx));  // a stale error word is not this test's
-    CTB_LAUNCH(ctx, launch_wait_selftest(polls, ctx->d_err, ctx->stream));
+    CTB_LAUNCH(ctx, launch_wait_selftest(limit_us, ctx->d_err, ctx->stream));
     return check_error_word(ctx);
 }
 

@@ -115,6 +115,11 @@ cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int
                            int na, int nd, Trig trig, const int4* d_groups, int ngroups,
                            const int* d_order, const int4* d_box, const int2* d_band, float* d_sino,
                            cudaStream_t st);
+// Twiddle tables of the filter's FFT of length L (every radix-16 pass and the
+// radix-2/4/8 last pass, r-major per pass), correctly rounded from double
+// precision; fft_twiddle_len(L) entries.
+size_t fft_twiddle_len(int L);
+std::vector<float2> fft_twiddle_table(int L);
 cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
                           const FiltLayout& fl, const float2* d_Hc, const float2* d_tw,
                           const float4* d_stats, int denorm, float scale, float4* d_filt,
@@ -182,7 +187,7 @@ struct FiltBatch {
     int njobs = 0;
     int Lc = 0;
     long long total = 0;
-    const float2* tw = nullptr;  // exp(-2 pi i k / Lc)
+    const float2* tw = nullptr;  // fft_twiddle_table(Lc)
     FiltJob job[kMaxJobs];
 };
 // Conventions of a reconstruction: SerialBackend's (the default, the oracle)
@@ -203,10 +208,10 @@ cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltL
                                int n_out, Trig trig, const float4* d_stats, int denorm,
                                float* d_out, unsigned* d_err, cudaStream_t st, int variant = 0,
                                int convention = kConvSerial);
-// One CTA whose threads wait, at most `polls` polls each, on an mbarrier that
-// nothing completes; each records a timeout in *d_err (the timeout path's
-// self-test).
-cudaError_t launch_wait_selftest(unsigned polls, unsigned* d_err, cudaStream_t st);
+// One CTA whose threads wait, at most `limit_us` microseconds each, on an
+// mbarrier that nothing completes; each records a timeout in *d_err (the
+// timeout path's self-test).
+cudaError_t launch_wait_selftest(unsigned limit_us, unsigned* d_err, cudaStream_t st);
 cudaError_t launch_point_count(const float* d_vol, long long total, float thr,
                                unsigned* d_block_counts, int blocks, cudaStream_t st);
 cudaError_t launch_point_write(const float* d_vol, int nx, int ny, long long total, float thr,

@@ -19,11 +19,13 @@
 // launch filters any number of sinogram stacks that share Lc. The FFT is a
 // radix-16 Stockham transform (one
 // radix-2/4/8 pass when log2 L is not a multiple of 4) with twiddles read
-// from a double-precision-accurate table. The last inverse pass writes its
-// natural-order samples straight to the output rows, float4 per bin (one
+// from per-pass tables of correctly rounded values laid out so that the
+// threads of a warp read consecutive entries (fft_twiddle_table). The last
+// inverse pass writes its natural-order samples straight to the output rows, float4 per bin (one
 // value per slice), the layout the backprojector stages, scaled by
 // pi/(2 na) times the slice's denormalisation span.
 #include <cmath>
+#include <vector>
 
 #include "ctb_internal.h"
 
@@ -36,6 +38,10 @@ __device__ __forceinline__ int padi(int p) { return p + (p >> 4); }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
 }
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -122,31 +128,25 @@ __device__ __forceinline__ void dft(float2* v) {
     else dft16<INV>(v);
 }
 
-// Twiddles w[r] = exp(-+2 pi i r m / L) = tw[r m], r = 0..15, for a radix-16
-// butterfly: six table loads (r = 1, 2, 3, 4, 8, 12), the other nine as one
-// product each (w[4a + b] = w[4a] w[b]).
+// Twiddle tables. A Stockham pass of radix R that combines sub-transforms of
+// length Ns multiplies input r of butterfly k (k = j mod Ns) by
+// w = exp(-2 pi i r k / (Ns R)) (the conjugate in the inverse transform). The
+// values of one (R, Ns) pair are stored r-major, entry (r - 1) Ns + k, so the
+// lanes of a warp (consecutive j, hence consecutive k) read consecutive
+// entries. Radix-16 tables for every Ns = 2^i < L/16 ... L/16 sit at
+// 15 (Ns - 1); the table of a radix-2/4/8 last pass (Ns = L/R) follows at
+// 15 (L/8 - 1). Both transforms of a row use the same tables.
+__device__ __forceinline__ int tw16_offset(int Ns) { return 15 * (Ns - 1); }
+__device__ __forceinline__ int twr_offset(int L) { return 15 * (L / 8 - 1); }
+
 template <bool INV>
-__device__ __forceinline__ void twiddles16(const float2* __restrict__ tw, int m, float2 (&w)[16]) {
-    w[0] = make_float2(1.0f, 0.0f);
-    w[1] = __ldg(tw + m);
-    w[2] = __ldg(tw + 2 * m);
-    w[3] = __ldg(tw + 3 * m);
-    w[4] = __ldg(tw + 4 * m);
-    w[8] = __ldg(tw + 8 * m);
-    w[12] = __ldg(tw + 12 * m);
-#pragma unroll
-    for (int a = 4; a <= 12; a += 4)
-#pragma unroll
-        for (int b = 1; b < 4; ++b) w[a + b] = cmul(w[a], w[b]);
-    if (INV) {
-#pragma unroll
-        for (int r = 1; r < 16; ++r) w[r].y = -w[r].y;
-    }
+__device__ __forceinline__ float2 twiddle_mul(float2 v, float2 w) {
+    return INV ? cmulc(v, w) : cmul(v, w);
 }
 
 // One Stockham pass of radix R over a length-L sequence in shared memory,
 // executed by T = L/(16 K) threads (16 K / R butterflies each). Ns is the
-// length of the sub-transforms already combined. tw[i] = exp(-2 pi i i / L).
+// length of the sub-transforms already combined; tw holds the twiddle tables.
 template <int R, bool INV, int K>
 __device__ __forceinline__ void stockham_pass(float2* buf, int L, int Ns, int tid, int T,
                                               const float2* __restrict__ tw) {
@@ -160,20 +160,10 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int L, int Ns, int ti
 #pragma unroll
         for (int r = 0; r < R; ++r) v[bi][r] = buf[padi(j + r * LR)];
         if (Ns > 1) {
-            const int step = L / (Ns * R);
-            if constexpr (R == 16) {
-                float2 w[16];
-                twiddles16<INV>(tw, k * step, w);
+            static_assert(R == 16, "inner passes are radix 16");
+            const float2* t = tw + tw16_offset(Ns) + k;
 #pragma unroll
-                for (int r = 1; r < 16; ++r) v[bi][r] = cmul(v[bi][r], w[r]);
-            } else {
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    float2 w = __ldg(tw + r * k * step);
-                    if (INV) w.y = -w.y;
-                    v[bi][r] = cmul(v[bi][r], w);
-                }
-            }
+            for (int r = 1; r < 16; ++r) v[bi][r] = twiddle_mul<INV>(v[bi][r], __ldg(t + (r - 1) * Ns));
         }
         dft<R, INV>(v[bi]);
     }
@@ -212,20 +202,9 @@ __device__ __forceinline__ void last_pass_out(const float2* buf, int L, int tid,
 #pragma unroll
         for (int r = 0; r < R; ++r) v[bi][r] = buf[padi(j + r * LR)];
         if (LR > 1) {
-            const int step = 1;  // L / (Ns R)
-            if constexpr (R == 16) {
-                float2 w[16];
-                twiddles16<true>(tw, j * step, w);
+            const float2* t = tw + (R == 16 ? tw16_offset(LR) : twr_offset(L)) + j;
 #pragma unroll
-                for (int r = 1; r < 16; ++r) v[bi][r] = cmul(v[bi][r], w[r]);
-            } else {
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    float2 w = __ldg(tw + r * j * step);
-                    w.y = -w.y;
-                    v[bi][r] = cmul(v[bi][r], w);
-                }
-            }
+            for (int r = 1; r < R; ++r) v[bi][r] = cmulc(v[bi][r], __ldg(t + (r - 1) * LR));
         }
         dft<R, true>(v[bi]);
 #pragma unroll
@@ -282,10 +261,9 @@ __device__ __forceinline__ void fused_middle(float2* buf, int L, int tid, int T,
 #pragma unroll
         for (int r = 0; r < 16; ++r) v[bi][r] = buf[padi(j + r * LR)];
         if (LR > 1) {
-            float2 w[16];
-            twiddles16<false>(tw, j, w);
+            const float2* t = tw + tw16_offset(LR) + j;
 #pragma unroll
-            for (int r = 1; r < 16; ++r) v[bi][r] = cmul(v[bi][r], w[r]);
+            for (int r = 1; r < 16; ++r) v[bi][r] = cmul(v[bi][r], __ldg(t + (r - 1) * LR));
         }
         dft16<false>(v[bi]);
 #pragma unroll
@@ -392,6 +370,34 @@ __global__ void __launch_bounds__(256, (K == 1 ? 3 : 1)) k_filter(const __grid_c
 }
 
 }  // namespace
+
+size_t fft_twiddle_len(int L) {
+    int logL = 0;
+    while ((1 << logL) < L) ++logL;
+    const int rem = logL & 3;
+    const size_t n16 = 15 * static_cast<size_t>(L / 8 - 1);  // radix-16 tables, Ns = 1 .. L/16
+    return rem == 0 ? n16 : n16 + static_cast<size_t>((1 << rem) - 1) * (L >> rem);
+}
+
+std::vector<float2> fft_twiddle_table(int L) {
+    std::vector<float2> t(fft_twiddle_len(L), make_float2(1.0f, 0.0f));
+    auto put = [&](size_t off, int R, int Ns) {
+        for (int r = 1; r < R; ++r)
+            for (int k = 0; k < Ns; ++k) {
+                // exp(-2 pi i r k / (Ns R)), argument reduced exactly in integers
+                const long long m = (static_cast<long long>(r) * k) % (static_cast<long long>(Ns) * R);
+                const double a = 2.0 * 3.14159265358979323846 * static_cast<double>(m) / (static_cast<double>(Ns) * R);
+                t[off + static_cast<size_t>(r - 1) * Ns + k] =
+                    make_float2(static_cast<float>(std::cos(a)), static_cast<float>(-std::sin(a)));
+            }
+    };
+    for (int Ns = 1; Ns <= L / 16; Ns *= 2) put(15 * static_cast<size_t>(Ns - 1), 16, Ns);
+    int logL = 0;
+    while ((1 << logL) < L) ++logL;
+    const int rem = logL & 3;
+    if (rem) put(15 * static_cast<size_t>(L / 8 - 1), 1 << rem, L >> rem);
+    return t;
+}
 
 FiltJob make_filt_job(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
                       const float2* d_Hc, const float4* d_stats, int denorm, float scale,

@@ -37,7 +37,10 @@ constexpr size_t kOffAngles = 256;
 constexpr size_t kOffTrig = kOffAngles + sizeof(float) * kMaxAngles;           // double2 + float2
 constexpr size_t kOffHc = kOffTrig + (sizeof(double2) + sizeof(float2)) * kMaxAngles;
 constexpr size_t kOffTw = kOffHc + sizeof(float2) * kMaxConv;
-constexpr size_t kOffFilt = kOffTw + sizeof(float2) * kMaxConv;
+// FFT twiddle tables of the longest convolution (fft_twiddle_len(8192) =
+// 15 (8192/8 - 1) + 1 x 4096 entries), rounded up to 256 bytes
+constexpr size_t kTwEntries = 15 * (kMaxConv / 8 - 1) + kMaxConv / 2;
+constexpr size_t kOffFilt = kOffTw + (sizeof(float2) * kTwEntries + 255) / 256 * 256;
 constexpr size_t kFiltCapacity = (kScratchBytes - kOffFilt) / sizeof(float4);  // float4 bins
 static_assert(kOffTrig % 256 == 0 && kOffHc % 256 == 0 && kOffTw % 256 == 0 && kOffFilt % 256 == 0,
               "scratch layout must stay 256-byte aligned");
@@ -100,12 +103,11 @@ extern "C" ctb_status ctb_fbp_noalloc(const float* d_sino, int depth, int num_an
         csf[a] = make_float2(std::cos(th), std::sin(th));
     }
     const std::vector<double> Hd = conv_response(g, filter);
-    std::vector<float2> Hc(g.Lc), tw(g.Lc);
-    for (int k = 0; k < g.Lc; ++k) {
+    std::vector<float2> Hc(g.Lc);
+    for (int k = 0; k < g.Lc; ++k)
         Hc[k] = make_float2(static_cast<float>(Hd[2 * k]), static_cast<float>(Hd[2 * k + 1]));
-        const double ang = 2.0 * 3.14159265358979323846 * static_cast<double>(k) / g.Lc;
-        tw[k] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(-std::sin(ang)));
-    }
+    const std::vector<float2> tw = fft_twiddle_table(g.Lc);
+    if (tw.size() > kTwEntries) return CTB_ERR_UNSUPPORTED;
     unsigned* d_err = reinterpret_cast<unsigned*>(base + kOffErr);
     float* d_deg = reinterpret_cast<float*>(base + kOffAngles);
     double2* d_cs = reinterpret_cast<double2*>(base + kOffTrig);
@@ -118,7 +120,7 @@ extern "C" ctb_status ctb_fbp_noalloc(const float* d_sino, int depth, int num_an
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_deg, deg.data(), sizeof(float) * num_angles, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_csf, csf.data(), sizeof(float2) * num_angles, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_Hc, Hc.data(), sizeof(float2) * g.Lc, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_tw, tw.data(), sizeof(float2) * g.Lc, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = launch_trig(d_deg, num_angles, d_cs, st);
     const float scale = 3.14159265358979323846f / (2.0f * static_cast<float>(num_angles));
     if (e == cudaSuccess)

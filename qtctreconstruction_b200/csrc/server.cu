@@ -267,14 +267,10 @@ ctb_status request_tables(ctb_server* s, SReq* q) {
     }
     auto jt = s->twiddles.find(Lc);
     if (jt == s->twiddles.end()) {
-        std::vector<float2> tw(Lc);
-        for (int i = 0; i < Lc; ++i) {
-            const double ang = 2.0 * 3.14159265358979323846 * static_cast<double>(i) / Lc;
-            tw[i] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(-std::sin(ang)));
-        }
+        const std::vector<float2> tw = fft_twiddle_table(Lc);
         DevBuf b;
-        if (cudaMalloc(&b.ptr, sizeof(float2) * Lc) != cudaSuccess) return CTB_ERR_OOM;
-        b.bytes = sizeof(float2) * Lc;
+        if (cudaMalloc(&b.ptr, sizeof(float2) * tw.size()) != cudaSuccess) return CTB_ERR_OOM;
+        b.bytes = sizeof(float2) * tw.size();
         if (cudaMemcpyAsync(b.ptr, tw.data(), b.bytes, cudaMemcpyHostToDevice, s->table_stream) != cudaSuccess ||
             cudaStreamSynchronize(s->table_stream) != cudaSuccess) {
             cudaFree(b.ptr);

@@ -32,9 +32,12 @@ REL_L2 = 1e-5
 MAX_ABS = 1e-4
 
 # The static array: 16 MiB, of which the filtered rows get what the fixed
-# tables (error word, 2048 angles of degrees and trig, two spectra of 8192
-# complex values) leave, in float4 bins.
-FILT_CAPACITY = ((16 << 20) - (256 + 4 * 2048 + 24 * 2048 + 8 * 8192 + 8 * 8192)) // 16
+# tables leave, in float4 bins: the error word (256 B), 2048 angles of degrees
+# (4 B) and trig (24 B), the spectrum of an 8192-long convolution (8 B each)
+# and the FFT twiddle tables of that length (15 (8192/8 - 1) + 4096 complex
+# values, rounded up to 256 B).
+_TW_BYTES = (8 * (15 * (8192 // 8 - 1) + 8192 // 2) + 255) // 256 * 256
+FILT_CAPACITY = ((16 << 20) - (256 + 4 * 2048 + 24 * 2048 + 8 * 8192 + _TW_BYTES)) // 16
 
 
 def _pitch(bins, n_out):
