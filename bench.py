@@ -324,6 +324,26 @@ def cpu_native_rate(cfg: dict, slices: int, params, repeats: int = 3):
     return n * n * slices * na / statistics.median(times), threads
 
 
+def cpu_serial_rate(cfg: dict, slices: int, params, repeats: int = 3):
+    """The reference SerialBackend's own reconstructVolume (one thread, its
+    native path with detector bins = N) on `slices` central slices of the
+    phantom, median of `repeats` runs. Returns updates/s or None when the
+    reference build is absent."""
+    import oracle as O
+    from oracle import reference as R
+    lib, _ = R.timing_lib()
+    if lib is None:
+        return None
+    n, nz, na, kind = cfg["n"], cfg["nz"], cfg["na"], cfg["filter"]
+    vol = O.phantom_sum_slab(params, n, n, nz, nz // 2 - slices // 2, slices)
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        R.reconstruct_volume(R.SERIAL, vol, na, kind, lib=lib)
+        times.append(time.perf_counter() - t0)
+    return n * n * slices * na / statistics.median(times)
+
+
 def run_reference(args, cfg, rank: int, world: int):
     """--impl reference: the reference's CPU path, rank 0 only."""
     if rank != 0:
@@ -535,6 +555,14 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
                     "sample": f"{2 * args.ref_slices} central of {cfg['nz']} slices, "
                               "OpenMPBackend::reconstructVolume (its native volume path, detector bins = N), "
                               "median of 3 runs"}
+            ser_slices = cfg["nz"] if n <= 128 else 2
+            ser = cpu_serial_rate(cfg, ser_slices, params)
+            if ser:
+                line["cpu_baseline_serial"] = {
+                    "value": ser, "unit": UNIT, "cores": 1, "kind": "reference",
+                    "volume_s": n * n * nz * na / ser,
+                    "sample": f"{ser_slices} of {cfg['nz']} slices, SerialBackend::reconstructVolume (one thread, "
+                              "detector bins = N), median of 3 runs; volume_s scales it to the whole volume"}
         print(json.dumps(line), flush=True)
     be.close()
     if dist is not None:
@@ -720,7 +748,8 @@ def serving_shapes(seed: int, count: int, big_fraction: float):
 
 
 def run_plain_stream(be, reqs, arrivals):
-    """One request per call (ctb_fbp on host buffers), in arrival order."""
+    """One request per call (ctb_fbp on host buffers: slab-streamed copies
+    overlapped with the request's own compute), in arrival order."""
     lat, t0 = [], time.perf_counter()
     for r, a in zip(reqs, arrivals):
         now = time.perf_counter() - t0
@@ -750,6 +779,34 @@ def run_served_stream(ctb, reqs, arrivals, budget: int, copy_threads: int):
     return st
 
 
+def run_plain_device(be, dev):
+    """Device-resident requests, one per call: ctb_fbp_d then a synchronise
+    (the call returns when the request is done), back to back."""
+    import torch
+    lat = []
+    t0 = time.perf_counter()
+    for d in dev:
+        s = d["shape"]
+        t1 = time.perf_counter()
+        be.fbp_d(d["sino"].data_ptr(), s["nz"], s["na"], s["nd"], s["n"], s["filter"], d["out"].data_ptr())
+        be.synchronize()
+        lat.append((time.perf_counter() - t1) * 1e3)
+    torch.cuda.synchronize()
+    return lat, time.perf_counter() - t0
+
+
+def run_served_device(ctb, dev, budget: int):
+    """The same device-resident requests submitted at once to ctb_server
+    (CTB_REQ_DEVICE: nothing is staged; requests are batched)."""
+    with ctb.Server(0, memory_budget=budget) as srv:
+        ids = [srv.submit_device(d["sino"].data_ptr(), d["shape"]["nz"], d["shape"]["na"], d["shape"]["nd"],
+                                 d["shape"]["n"], d["shape"]["filter"], d["out"].data_ptr()) for d in dev]
+        status = [srv.wait(i) for i in ids]
+        st = srv.stats()
+    assert all(s == 0 for s in status), status
+    return st
+
+
 def percentile(v, p):
     v = sorted(v)
     return v[min(len(v) - 1, max(0, math.ceil(p * len(v)) - 1))]
@@ -757,11 +814,16 @@ def percentile(v, p):
 
 def run_serving(args, cfg, rank: int, world: int, local: int):
     """Config "serving": a Poisson stream of FBP requests (90 % the batch mix,
-    10 % 1024^2 x 64 x 1440) served two ways on the same GPU from the same host
-    buffers: the plain backend (ctb_fbp, one request per call) and ctb_server
-    (continuous batching, memory-budgeted admission, staged copies). First both
-    at saturation (all requests present at t = 0), then at arrival rates given
-    as multiples of the plain backend's saturated rate."""
+    10 % 1024^2 x 64 x 1440) served two ways on the same GPU from the same
+    page-locked host buffers: the plain backend (ctb_fbp, one request per
+    call, each call streaming its own slabs with copies overlapped) and
+    ctb_server (continuous batching, memory-budgeted admission, copies of
+    other requests overlapped). First both at saturation (all requests present
+    at t = 0), then at arrival rates given as multiples of the plain backend's
+    saturated rate. Then the same requests device-resident (sinograms already
+    in HBM, volumes left there): one ctb_fbp_d call per request against the
+    server's batches, which isolates what batching itself gains from what
+    overlapping the host copies gains."""
     import numpy as np
     import torch
 
@@ -769,8 +831,9 @@ def run_serving(args, cfg, rank: int, world: int, local: int):
     torch.cuda.set_device(local)
     be = ctb.B200Backend(local)
     shapes = serving_shapes(cfg["seed"], cfg["requests"], cfg["big_fraction"])
-    # sinograms of seeded phantoms, forward-projected on the GPU, kept in host memory
-    reqs = []
+    # sinograms of seeded phantoms, forward-projected on the GPU, kept in
+    # page-locked host memory (both arms read and write the same buffers)
+    reqs, pinned = [], []
     for k, s in enumerate(shapes):
         n, nz, na, nd = s["n"], s["nz"], s["na"], s["nd"]
         vol = torch.empty((nz, n, n), dtype=torch.float32, device="cuda")
@@ -779,8 +842,11 @@ def run_serving(args, cfg, rank: int, world: int, local: int):
         stats = torch.empty((nz, 4), dtype=torch.float32, device="cuda")
         be.forward_d(vol.data_ptr(), n, nz, na, nd, sino.data_ptr(), stats.data_ptr())
         be.synchronize()
-        # np.full writes every page now: no first-touch page faults inside a timed run
-        reqs.append(dict(shape=s, sino=sino.cpu().numpy(), out=np.full((nz, n, n), 0.0, np.float32)))
+        hs = torch.empty((nz, na, nd), dtype=torch.float32, pin_memory=True)
+        hs.copy_(sino)
+        ho = torch.zeros((nz, n, n), dtype=torch.float32, pin_memory=True)  # pages touched now
+        pinned.append((hs, ho))
+        reqs.append(dict(shape=s, sino=hs.numpy(), out=ho.numpy()))
         del vol, sino
     torch.cuda.empty_cache()
     count = len(reqs)
@@ -818,6 +884,15 @@ def run_serving(args, cfg, rank: int, world: int, local: int):
                                 "p99_ms": percentile(lp, 0.99)},
                       "served": {"volumes_per_s": ss["volumes_per_s"], "p50_ms": ss["p50_ms"],
                                  "p99_ms": ss["p99_ms"], "mean_batch": ss["mean_batch"]}})
+    # device-resident: the same requests with sinograms and volumes in HBM
+    dev = [dict(shape=r["shape"], sino=torch.from_numpy(r["sino"]).cuda(),
+                out=torch.zeros(r["out"].shape, dtype=torch.float32, device="cuda")) for r in reqs]
+    run_plain_device(be, dev[:args.warmup])
+    run_served_device(ctb, dev[:args.warmup], budget)
+    lat_d, span_d = run_plain_device(be, dev)
+    ref_d = [d["out"].cpu() for d in dev[:3]]
+    st_d = run_served_device(ctb, dev, budget)
+    same_d = all(torch.equal(a, d["out"].cpu()) for a, d in zip(ref_d, dev[:3]))
     clocks = sampler.stop()
     line = {
         "metric": "volumes/s (mixed FBP request stream)", "value": served_sat, "unit": "volumes/s",
@@ -825,16 +900,24 @@ def run_serving(args, cfg, rank: int, world: int, local: int):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "serving", "description": cfg["name"], "requests": count,
                    "voxels": vol_bytes // 4, "sinogram_bytes": sino_bytes, "budget_bytes": budget,
-                   "copy_threads": cfg["copy_threads"], "l2": "inputs larger than L2, no flush"},
+                   "copy_threads": cfg["copy_threads"], "host_buffers": "page-locked, shared by both arms",
+                   "l2": "inputs larger than L2, no flush"},
         "served": {"volumes_per_s": served_sat, "updates_per_s": st["updates_per_s"], "p50_ms": st["p50_ms"],
                    "p99_ms": st["p99_ms"], "batches": st["batches"], "mean_batch": st["mean_batch"],
                    "memory_peak": st["memory_peak"]},
         "plain": {"volumes_per_s": plain_sat, "updates_per_s": updates / span_p,
                   "p50_ms": percentile(lat_p, 0.5), "p99_ms": percentile(lat_p, 0.99),
-                  "api": "ctb_fbp, one request per call"},
+                  "api": "ctb_fbp, one request per call, slab-streamed copies overlapped with its compute"},
         "served_vs_plain": served_sat / plain_sat,
         "outputs_identical": same,
         "sweep": sweep,
+        "device_resident": {
+            "plain": {"volumes_per_s": count / span_d, "p50_ms": percentile(lat_d, 0.5),
+                      "p99_ms": percentile(lat_d, 0.99), "api": "ctb_fbp_d + synchronise per request"},
+            "served": {"volumes_per_s": st_d["volumes_per_s"], "p50_ms": st_d["p50_ms"], "p99_ms": st_d["p99_ms"],
+                       "batches": st_d["batches"], "mean_batch": st_d["mean_batch"]},
+            "served_vs_plain": st_d["volumes_per_s"] / (count / span_d),
+            "outputs_identical": same_d},
         "e2e": {"value": served_sat, "unit": "volumes/s", "h2d_bytes_per_step": sino_bytes // count,
                 "d2h_bytes_per_step": vol_bytes // count},
         "clocks": clocks,

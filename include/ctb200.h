@@ -326,11 +326,17 @@ void ctb_batch_destroy(ctb_batch* batch);
 /* ctb_batch_create + run + synchronise + destroy. */
 ctb_status ctb_fbp_batch_d(ctb_ctx* ctx, const ctb_fbp_job* jobs, int njobs);
 
-/* Plain one-request-per-call FBP on host buffers: copy sinos[depth][na][bins]
- * to the device, filter + backproject into output_size^2 slices (normalised
- * units), copy the result to out[depth][output_size]^2; returns when done.
- * The reference's reconstructVolumeFromSinograms with an explicit output size
- * (BackendFactory.cpp:17-60 reconstructs slice by slice). */
+/* Plain one-request-per-call FBP on host buffers: sinos[depth][na][bins] are
+ * filtered and backprojected into out[depth][output_size]^2 (normalised
+ * units); returns when done. The stack is streamed in slabs of slices: the
+ * next slab's sinograms copy in and the previous slab's slices copy out on
+ * their own streams while the current slab is computed (the reference's CUDA
+ * backend likewise pipelines pinned copies on two streams, CUDABackend.cu:
+ * 370-452,739-863). Copies overlap fully only from page-locked host memory.
+ * The result equals one pass over the whole stack bit for bit. The
+ * reference's reconstructVolumeFromSinograms with an explicit output size
+ * (BackendFactory.cpp:17-60 reconstructs slice by slice);
+ * ctb_reconstruct_from_sinograms runs the same pipeline. */
 ctb_status ctb_fbp(ctb_ctx* ctx, const float* sinos, int depth, int num_angles, int bins,
                    const float* angles_deg, int output_size, int filter, float* out);
 
@@ -340,11 +346,13 @@ ctb_status ctb_fbp(ctb_ctx* ctx, const float* sinos, int depth, int num_angles, 
  * different sizes, angle counts and filters are submitted at any time; a
  * scheduler thread admits them in arrival order while their device footprint
  * (sinograms, angle table, filtered rows, volume) fits the memory budget, copy
- * threads stage host data through pinned buffers on their own streams, and
- * every scheduling iteration packs the requests whose data is on the device
- * into one batch (ctb_batch semantics: one filter launch per convolution
- * length, one persistent backprojection launch) while other requests upload
- * and download. Results are bit-identical to ctb_fbp_d on the same request. */
+ * threads move host data on their own streams (directly from page-locked
+ * memory, else through pinned staging buffers), and every scheduling
+ * iteration packs the requests whose data is on the device into one batch
+ * (ctb_batch semantics: one filter launch per convolution length, one
+ * backprojection launch per tile shape over all the batch's (request, slice
+ * group, tile) items) while other requests upload and download. Results are
+ * bit-identical to ctb_fbp_d on the same request. */
 typedef struct ctb_server ctb_server;
 
 typedef struct ctb_server_config {

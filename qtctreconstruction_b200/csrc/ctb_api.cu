@@ -358,6 +358,160 @@ ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins
     return CTB_OK;
 }
 
+// Slabs of a host-buffer pipeline: {first slice, slices}, whole 8-slice
+// groups (the forward projector's groups, and whole 4-slice groups of the
+// filter and backprojector, so that a slab-streamed result equals one pass
+// over the whole stack bit for bit), about depth/8 slices each. The host->device
+// copy of slab k + 1 and the device->host copy of slab k - 1 run on their own
+// streams while slab k is computed. The schedule tapers at both ends (a
+// quarter slab, three quarters, double slabs, three quarters, a quarter), so
+// the copy in before the first slab and the copy out after the last one,
+// which nothing overlaps, are short, while the middle launches are large
+// enough to keep their tail waves small; each copy in stays shorter than the
+// slab computed beside it.
+std::vector<int2> plan_slabs(int depth) {
+    constexpr int kSlabs = 8;
+    std::vector<int2> slabs;
+    if (depth <= 16) {
+        slabs.push_back(make_int2(0, depth));
+        return slabs;
+    }
+    const int slab = 8 * ((depth + 8 * kSlabs - 1) / (8 * kSlabs));
+    const int rem = depth % 8;  // a partial last group goes at the very end
+    const int body = depth - rem;
+    const int q = slab >= 32 ? 8 * (slab / 32) : 0;  // a quarter slab, whole groups
+    std::vector<int> head, tail;
+    if (q > 0 && body >= 4 * slab) {
+        head = {q, slab - q};
+        tail = {slab - q, q};
+    }
+    int left = body;
+    for (int h : head) left -= h;
+    for (int h : tail) left -= h;
+    int z = 0;
+    for (int h : head) { slabs.push_back(make_int2(z, h)); z += h; }
+    const int big = head.empty() ? slab : 2 * slab;
+    while (left > 0) {
+        const int m = std::min(big, left);
+        slabs.push_back(make_int2(z, m));
+        z += m;
+        left -= m;
+    }
+    for (int h : tail) { slabs.push_back(make_int2(z, h)); z += h; }
+    if (rem > 0) {
+        if (!slabs.empty() && slabs.back().y + rem <= slab) slabs.back().y += rem;
+        else slabs.push_back(make_int2(z, rem));
+    }
+    return slabs;
+}
+
+// Host-buffer FBP of a sinogram stack sinos[depth][na][bins] into
+// out[depth][n_out]^2, streamed in slabs (plan_slabs): slab k + 1's sinograms
+// copy in on one stream and slab k - 1's slices copy out on another while slab
+// k is filtered and backprojected on the context's stream; two buffers each
+// way. With denorm != NONE each slice's min/max come from its own sinogram,
+// as the interface's default reconstructVolumeFromSinograms takes them
+// (BackendFactory.cpp:41-51). The result equals one pass over the whole stack
+// bit for bit (whole 8-slice slabs, the tile shape chosen for the whole
+// depth). Copies run at full speed only from page-locked host memory; from
+// pageable memory the driver stages them. Sets last_recon_ms to the device
+// time from the first slab's compute to the last one's.
+ctb_status fbp_host_pipeline(ctb_ctx* ctx, const float* sinos, int depth, int na, int bins,
+                             const float* angles_deg, int n_out, int filter, int denorm, float* out) {
+    const std::vector<int2> slabs = plan_slabs(depth);
+    const int nslab = static_cast<int>(slabs.size());
+    int slab = 0;
+    for (const int2& sl : slabs) slab = std::max(slab, sl.y);
+    const size_t row = static_cast<size_t>(na) * bins, img = static_cast<size_t>(n_out) * n_out;
+    const PadGeom g = pad_geometry(bins);
+    if (g.Lc > kMaxFft)
+        return fail(ctx, CTB_ERR_UNSUPPORTED, "convolution length %d (bins %d) exceeds %d", g.Lc, bins, kMaxFft);
+    CTB_WS(ctx, d_sino, float, "h_sino", 2 * static_cast<size_t>(slab) * row);
+    CTB_WS(ctx, d_out, float, "h_out", 2 * static_cast<size_t>(slab) * img);
+    CTB_WS(ctx, d_stats, float4, "h_stats", 2 * static_cast<size_t>(slab));
+    {  // the filter stage's workspaces at their final size: nothing reallocates mid-pipeline
+        const FiltLayout fl = filt_layout(g.sq, n_out);
+        CTB_WS(ctx, d_filt, float4, "filt", static_cast<size_t>((slab + 3) / 4) * na * fl.pitch);
+        (void)d_filt;
+        if (ctx->filter_mode == CTB_FILTER_MODE_TC_BF16X3) {
+            CTB_WS(ctx, d_split, unsigned char, "gemm_split", filter_gemm_split_bytes(slab, na, bins));
+            (void)d_split;
+        }
+    }
+    // tables first: building them synchronises the context's stream
+    Trig trig;
+    CTB_TRY(trig_table(ctx, angles_deg, na, &trig));
+    const float2* d_Hc = nullptr;
+    const float2* d_tw = nullptr;
+    CTB_TRY(filter_tables(ctx, g, filter, &d_Hc, &d_tw, ctx->convention == kConvCuda));
+    if (!ctx->copy_in) {
+        CTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
+        CTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
+    }
+    // events: per buffer {sinograms landed, FBP done (sinograms read, slices
+    // ready), slices copied out}; then first and last compute marks
+    while (ctx->slab_ev.size() < 8) {
+        cudaEvent_t e;
+        CTB_CUDA(ctx, cudaEventCreate(&e));
+        ctx->slab_ev.push_back(e);
+    }
+    cudaEvent_t* in_done = &ctx->slab_ev[0];
+    cudaEvent_t* fbp_done = &ctx->slab_ev[2];
+    cudaEvent_t* out_done = &ctx->slab_ev[4];
+    cudaEvent_t* mark = &ctx->slab_ev[6];
+    cudaStream_t comp = ctx->stream;
+    for (int b = 0; b < 2; ++b) {  // buffers start free, after the caller's prior work
+        CTB_CUDA(ctx, cudaEventRecord(fbp_done[b], comp));
+        CTB_CUDA(ctx, cudaEventRecord(out_done[b], comp));
+    }
+    // an exit before the end first drains the three streams: no queued copy
+    // may still touch the caller's buffers once the call has returned
+    struct Drain {
+        ctb_ctx* c;
+        cudaStream_t comp;
+        bool finished = false;
+        ~Drain() {
+            if (!finished) {
+                cudaStreamSynchronize(c->copy_in);
+                cudaStreamSynchronize(comp);
+                cudaStreamSynchronize(c->copy_out);
+            }
+        }
+    } drain{ctx, comp};
+    for (int k = 0; k < nslab; ++k) {
+        const int b = k & 1;
+        const int z0 = slabs[k].x, nz = slabs[k].y;
+        float* sino_b = d_sino + static_cast<size_t>(b) * slab * row;
+        float* out_b = d_out + static_cast<size_t>(b) * slab * img;
+        float4* stats_b = d_stats + static_cast<size_t>(b) * slab;
+        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_in, fbp_done[b], 0));  // FBP k - 2 read sino_b
+        CTB_CUDA(ctx, cudaMemcpyAsync(sino_b, sinos + static_cast<size_t>(z0) * row, sizeof(float) * nz * row,
+                                      cudaMemcpyHostToDevice, ctx->copy_in));
+        CTB_CUDA(ctx, cudaEventRecord(in_done[b], ctx->copy_in));
+        CTB_CUDA(ctx, cudaStreamWaitEvent(comp, in_done[b], 0));
+        CTB_CUDA(ctx, cudaStreamWaitEvent(comp, out_done[b], 0));  // slab k - 2 copied out of out_b
+        if (k == 0) CTB_CUDA(ctx, cudaEventRecord(mark[0], comp));
+        if (denorm != CTB_DENORM_NONE)
+            CTB_LAUNCH(ctx, launch_slice_stats(sino_b, static_cast<long long>(row), nz, stats_b, comp));
+        CTB_TRY(fbp_stage(ctx, sino_b, nz, na, bins, angles_deg, n_out, filter,
+                          denorm != CTB_DENORM_NONE ? stats_b : nullptr, denorm, out_b, nullptr, depth));
+        CTB_CUDA(ctx, cudaEventRecord(fbp_done[b], comp));
+        CTB_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, fbp_done[b], 0));
+        CTB_CUDA(ctx, cudaMemcpyAsync(out + static_cast<size_t>(z0) * img, out_b, sizeof(float) * nz * img,
+                                      cudaMemcpyDeviceToHost, ctx->copy_out));
+        CTB_CUDA(ctx, cudaEventRecord(out_done[b], ctx->copy_out));
+    }
+    CTB_CUDA(ctx, cudaEventRecord(mark[1], comp));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->copy_out));
+    CTB_CUDA(ctx, cudaStreamSynchronize(comp));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->copy_in));
+    drain.finished = true;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, mark[0], mark[1]);
+    ctx->last_recon_ms = ms;
+    return check_error_word(ctx);
+}
+
 ctb_status check_common(ctb_ctx* ctx) {
     if (!ctx) return CTB_ERR_INVALID;
     return CTB_OK;
@@ -763,49 +917,9 @@ ctb_status ctb_reconstruct_volume(ctb_ctx* ctx, const float* vol, int n, int dep
         num_angles > kMaxAngles)
         return fail(ctx, CTB_ERR_INVALID, "ctb_reconstruct_volume: invalid arguments");
     Guard g(ctx);
-    // Slabs of whole 8-slice groups (the projector's groups, so the result is
-    // bit for bit that of one pass over the volume): the host->device copy of
-    // slab k + 1 and the device->host copy of slab k - 1 run on their own
-    // streams while slab k is reconstructed. Two slab buffers each way. The
-    // schedule tapers at both ends (a quarter slab, three quarters, double
-    // slabs, three quarters, a quarter), so the copy in before the first slab
-    // and the copy out after the last one, which nothing overlaps, are short,
-    // while the middle launches are large enough to keep their tail waves
-    // small; each copy in stays shorter than the slab computed beside it.
-    constexpr int kSlabs = 8;
-    std::vector<int2> slabs;  // {first slice, slices}
-    int slab = depth;
-    if (depth <= 16) {
-        slabs.push_back(make_int2(0, depth));
-    } else {
-        slab = 8 * ((depth + 8 * kSlabs - 1) / (8 * kSlabs));
-        const int rem = depth % 8;  // a partial last group goes at the very end
-        const int body = depth - rem;
-        const int q = slab >= 32 ? 8 * (slab / 32) : 0;  // a quarter slab, whole groups
-        std::vector<int> head, tail;
-        if (q > 0 && body >= 4 * slab) {
-            head = {q, slab - q};
-            tail = {slab - q, q};
-        }
-        int left = body;
-        for (int h : head) left -= h;
-        for (int h : tail) left -= h;
-        int z = 0;
-        for (int h : head) { slabs.push_back(make_int2(z, h)); z += h; }
-        const int big = head.empty() ? slab : 2 * slab;
-        while (left > 0) {
-            const int m = std::min(big, left);
-            slabs.push_back(make_int2(z, m));
-            z += m;
-            left -= m;
-        }
-        for (int h : tail) { slabs.push_back(make_int2(z, h)); z += h; }
-        if (rem > 0) {
-            if (!slabs.empty() && slabs.back().y + rem <= slab) slabs.back().y += rem;
-            else slabs.push_back(make_int2(z, rem));
-        }
-    }
+    const std::vector<int2> slabs = plan_slabs(depth);
     const int nslab = static_cast<int>(slabs.size());
+    int slab = 0;  // the largest slab: buffer sizes
     for (const int2& sl : slabs) slab = std::max(slab, sl.y);
     const size_t per = static_cast<size_t>(slab) * n * n;
     const size_t per_sino = static_cast<size_t>(slab) * num_angles * detector_bins;
@@ -921,29 +1035,11 @@ ctb_status ctb_reconstruct_from_sinograms(ctb_ctx* ctx, const float* sinos, int 
                                           int filter, int denorm, float* out) {
     CTB_TRY(check_common(ctx));
     if (!sinos || !out || !angles_deg || depth <= 0 || num_angles <= 0 || bins <= 0 ||
-        denorm < 0 || denorm > CTB_DENORM_CUDA)
+        num_angles > kMaxAngles || denorm < 0 || denorm > CTB_DENORM_CUDA)
         return fail(ctx, CTB_ERR_INVALID, "ctb_reconstruct_from_sinograms: invalid arguments");
     Guard g(ctx);
-    const size_t ns = static_cast<size_t>(depth) * num_angles * bins;
-    const size_t no = static_cast<size_t>(depth) * bins * bins;
-    CTB_WS(ctx, d_sino, float, "h_sino", ns);
-    CTB_WS(ctx, d_out, float, "h_out", no);
-    CTB_WS(ctx, d_stats, float4, "h_stats", depth);
-    CTB_CUDA(ctx, cudaMemcpyAsync(d_sino, sinos, ns * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
-    if (denorm != CTB_DENORM_NONE)  // BackendFactory.cpp:41-51: min/max of the sinogram itself
-        CTB_LAUNCH(ctx, launch_slice_stats(d_sino, static_cast<long long>(num_angles) * bins, depth,
-                                           d_stats, ctx->stream));
-    CTB_TRY(fbp_stage(ctx, d_sino, depth, num_angles, bins, angles_deg, bins, filter,
-                      denorm != CTB_DENORM_NONE ? d_stats : nullptr, denorm, d_out));
-    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
-    CTB_CUDA(ctx, cudaMemcpyAsync(out, d_out, no * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
-    ctx->last_recon_ms = ms;
     ctx->last_sino_ms = 0.0;
-    return check_error_word(ctx);
+    return fbp_host_pipeline(ctx, sinos, depth, num_angles, bins, angles_deg, bins, filter, denorm, out);
 }
 
 ctb_status ctb_fbp(ctb_ctx* ctx, const float* sinos, int depth, int num_angles, int bins,
@@ -953,21 +1049,8 @@ ctb_status ctb_fbp(ctb_ctx* ctx, const float* sinos, int depth, int num_angles, 
         output_size <= 0 || filter < 0 || filter > CTB_FILTER_BARTLETT)
         return fail(ctx, CTB_ERR_INVALID, "ctb_fbp: invalid arguments");
     Guard g(ctx);
-    const size_t ns = static_cast<size_t>(depth) * num_angles * bins;
-    const size_t no = static_cast<size_t>(depth) * output_size * output_size;
-    CTB_WS(ctx, d_sino, float, "h_sino", ns);
-    CTB_WS(ctx, d_out, float, "h_out", no);
-    CTB_CUDA(ctx, cudaMemcpyAsync(d_sino, sinos, ns * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
-    CTB_TRY(fbp_stage(ctx, d_sino, depth, num_angles, bins, angles_deg, output_size, filter, nullptr,
-                      CTB_DENORM_NONE, d_out));
-    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
-    CTB_CUDA(ctx, cudaMemcpyAsync(out, d_out, no * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
-    ctx->last_recon_ms = ms;
-    return check_error_word(ctx);
+    return fbp_host_pipeline(ctx, sinos, depth, num_angles, bins, angles_deg, output_size, filter,
+                             CTB_DENORM_NONE, out);
 }
 
 // ------------------------------------------------------------------ phantoms

@@ -9,14 +9,16 @@
 //               table, filtered rows, and unless the request is device-resident
 //               its sinograms and volume), then packs requests whose data is on
 //               the device into batches on the compute stream: one filter launch
-//               per convolution length and one persistent backprojection launch,
+//               per convolution length and one backprojection launch per tile
+//               shape over all (request, slice group, tile) items,
 //               at most two batches queued at a time so the GPU never waits for
 //               the host between batches.
-//   uploaders   fill a request's angle table and copy its host sinograms through
-//               a pinned double buffer on their own stream.
-//   downloaders copy finished volumes back through a pinned double buffer and
-//               release the request's arena block, which lets the scheduler admit
-//               the next requests.
+//   uploaders   fill a request's angle table and copy its host sinograms on
+//               their own stream: directly from page-locked memory, else
+//               through a pinned double buffer.
+//   downloaders copy finished volumes back the same way and release the
+//               request's arena block, which lets the scheduler admit the next
+//               requests.
 // A batch's completion is signalled by a host callback on the compute stream
 // (cudaLaunchHostFunc), which only touches host state. Requests that arrive
 // while others run join the next batch: continuous batching.
@@ -344,8 +346,9 @@ ctb_status launch_batch(ctb_server* s, const std::vector<SReq*>& reqs, int slot)
         }
         if (launch_filter_batch(f, s->compute) != cudaSuccess) return CTB_ERR_CUDA;
     }
-    // one persistent backprojection launch per tile shape (the default shape of
-    // each request, a function of its size), most angles first
+    // one backprojection launch per tile shape (the default shape of each
+    // request, a function of its size), one CTA per (request, slice group,
+    // tile) item, most angles first
     std::vector<int> var(n);
     for (int k = 0; k < n; ++k) var[k] = bp_default_variant(reqs[k]->r.output_size, reqs[k]->r.depth, s->sms);
     std::iota(order.begin(), order.end(), 0);
@@ -470,9 +473,25 @@ bool upload_trig(SReq* q, Stager& st) {
            cudaStreamSynchronize(st.stream) == cudaSuccess;
 }
 
-// Host -> device through the pinned double buffer: chunk k is copied into
-// buffer k & 1 once that buffer's previous transfer has finished.
+// A host buffer the copy engines can read or write directly (page-locked by
+// cudaHostAlloc or cudaHostRegister); pageable memory goes through the pinned
+// double buffers.
+bool page_locked(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Host -> device: straight from page-locked memory, else through the pinned
+// double buffer (chunk k is copied into buffer k & 1 once that buffer's
+// previous transfer has finished).
 bool staged_h2d(Stager& st, void* dst, const void* src, size_t bytes) {
+    if (page_locked(src))
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st.stream) == cudaSuccess &&
+               cudaStreamSynchronize(st.stream) == cudaSuccess;
     const char* s8 = static_cast<const char*>(src);
     char* d8 = static_cast<char*>(dst);
     int k = 0;
@@ -487,8 +506,12 @@ bool staged_h2d(Stager& st, void* dst, const void* src, size_t bytes) {
     return cudaStreamSynchronize(st.stream) == cudaSuccess;
 }
 
-// Device -> host: chunk k lands in buffer k & 1 while chunk k - 1 is copied out.
+// Device -> host: straight into page-locked memory, else chunk k lands in
+// buffer k & 1 while chunk k - 1 is copied out.
 bool staged_d2h(Stager& st, void* dst, const void* src, size_t bytes) {
+    if (page_locked(dst))
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st.stream) == cudaSuccess &&
+               cudaStreamSynchronize(st.stream) == cudaSuccess;
     const char* s8 = static_cast<const char*>(src);
     char* d8 = static_cast<char*>(dst);
     size_t prev_off = 0, prev_len = 0;
