@@ -20,9 +20,10 @@
 // (|u_local| < WIN): the interpolation position is ~10x more accurate than the
 // reference's float u of magnitude ~sq. Each of the 256 threads accumulates
 // VPT voxels x 4 slices in registers; voxels outside the circle load nothing.
-// Four tile shapes are compiled (32x32 / 4 per thread, the default; 64x32 / 8;
-// 32x16 / 2; 16x16 / 1); bp_default_variant picks one from the job's size, the
-// context's autotuner can time them per size bucket.
+// Six shapes are compiled: four tile shapes with 32-angle chunks (32x32 / 4
+// per thread, the default; 64x32 / 8; 32x16 / 2; 16x16 / 1) and the 32x32 tile
+// with 16- and 64-angle chunks; bp_default_variant picks one of the first four
+// from the job's size, the context's autotuner times all six per size bucket.
 //
 // One kernel serves both shapes of work: a single job with one CTA per item,
 // or a batch of jobs (BpBatch) on a persistent grid that takes items from an
@@ -58,6 +59,8 @@ using V0 = Shape<32, 32, 4, 32, 52, 4>;  // the general-purpose shape
 using V1 = Shape<64, 32, 8, 32, 76, 2>;  // wide tiles: half the staging per voxel
 using V2 = Shape<32, 16, 2, 32, 40, 4>;  // half-height tiles: twice the CTAs
 using V3 = Shape<16, 16, 1, 32, 28, 4>;  // small tiles for small slices
+using V4 = Shape<32, 32, 4, 16, 52, 4>;  // the general shape with 16-angle chunks (half the staging buffer)
+using V5 = Shape<32, 32, 4, 64, 52, 2>;  // the general shape with 64-angle chunks (half the chunk barriers)
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -430,6 +433,8 @@ BpShape bp_shape(int variant) {
     case 1: return shape_of<V1>();
     case 2: return shape_of<V2>();
     case 3: return shape_of<V3>();
+    case 4: return shape_of<V4>();
+    case 5: return shape_of<V5>();
     default: return shape_of<V0>();
     }
 }
@@ -503,6 +508,8 @@ cudaError_t launch_backproject_batch(const BpBatch& b, int variant, unsigned* d_
     case 1: return launch_many<V1>(b, persistent, d_counter, d_err, st);
     case 2: return launch_many<V2>(b, persistent, d_counter, d_err, st);
     case 3: return launch_many<V3>(b, persistent, d_counter, d_err, st);
+    case 4: return launch_many<V4>(b, persistent, d_counter, d_err, st);
+    case 5: return launch_many<V5>(b, persistent, d_counter, d_err, st);
     default: return launch_many<V0>(b, persistent, d_counter, d_err, st);
     }
 }
@@ -519,6 +526,8 @@ cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltL
     case 1: return launch_one<V1>(b, d_err, st);
     case 2: return launch_one<V2>(b, d_err, st);
     case 3: return launch_one<V3>(b, d_err, st);
+    case 4: return launch_one<V4>(b, d_err, st);
+    case 5: return launch_one<V5>(b, d_err, st);
     default: return launch_one<V0>(b, d_err, st);
     }
 }

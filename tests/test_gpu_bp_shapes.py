@@ -1,7 +1,8 @@
 """Backprojection tile shapes and the autotuner on the GPU.
 
 Every compiled shape must meet the parity bar against the oracle on sizes
-that are and are not multiples of its tile edges; the automatic choice is a
+that are and are not multiples of its tile edges; the shapes that differ
+only in angle-chunk size give identical bits; the automatic choice is a
 function of the job alone; the autotuner times the shapes on the first job of
 a size bucket, remembers the fastest, and its table can be exported and
 loaded; results stay within the parity tolerance whichever shape runs.
@@ -43,12 +44,13 @@ def _fbp(backend, torch, sinos, n, kind):
 
 
 def test_shape_info():
-    assert [ctb.bp_shape_info(v)[:3] for v in range(4)] == [(32, 32, 4), (64, 32, 8), (32, 16, 2), (16, 16, 1)]
+    assert [ctb.bp_shape_info(v) for v in range(6)] == [(32, 32, 4, 32), (64, 32, 8, 32), (32, 16, 2, 32),
+                                                        (16, 16, 1, 32), (32, 32, 4, 16), (32, 32, 4, 64)]
     with pytest.raises(ctb.CtbError):
-        ctb.bp_shape_info(4)
+        ctb.bp_shape_info(6)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("n,depth,na", [(64, 5, 90), (97, 3, 120), (200, 6, 150)])
 def test_every_shape_meets_parity(backend, variant, n, depth, na):
     import torch
@@ -65,6 +67,25 @@ def test_every_shape_meets_parity(backend, variant, n, depth, na):
         ref = O.reconstruct_slice_f32(sinos[z], ang, n, int(FilterType.Hann))
         assert O.rel_l2(got[z], ref) <= REL_L2
         assert O.max_abs_rel(got[z], ref) <= MAX_ABS
+
+
+@pytest.mark.parametrize("na", [17, 90, 150, 301])
+def test_angle_chunk_size_does_not_change_bits(backend, na):
+    """Shapes 4 and 5 are shape 0 with 16- and 64-angle chunks: every voxel
+    sums its angles in the same order, so the outputs are identical, also
+    when the angle count is not a multiple of the chunk."""
+    import torch
+    rng = np.random.default_rng(na)
+    sinos = _job(rng, 96, 5, na)
+    outs = []
+    for v in (0, 4, 5):
+        backend.set_bp_shape(v)
+        try:
+            outs.append(_fbp(backend, torch, sinos, 96, FilterType.SheppLogan))
+        finally:
+            backend.set_bp_shape(-1)
+    np.testing.assert_array_equal(outs[1], outs[0])
+    np.testing.assert_array_equal(outs[2], outs[0])
 
 
 def test_default_shape_depends_on_size_only(backend):
@@ -95,4 +116,4 @@ def test_autotune_table_round_trip(backend):
     for z in range(8):
         ref = O.reconstruct_slice_f32(sinos[z], ang, 160, int(FilterType.Ramp))
         assert O.rel_l2(got[z], ref) <= REL_L2
-    assert tuned in range(4)
+    assert tuned in range(6)
