@@ -676,7 +676,9 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
     One step = every job filtered and backprojected. Timed four ways on the
     same jobs: the batch replayed from a CUDA graph (the value), the batch
     launched directly, the batch with its backprojection on the persistent work
-    queue, and one filter + one backprojection launch per job."""
+    queue, and one filter + one backprojection launch per job. Then every
+    backprojection shape alone on three of the jobs, and the batch again with
+    the shapes the autotuner chose per size bucket."""
     import torch
 
     import qtctreconstruction_b200 as ctb
@@ -711,6 +713,46 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
                 results[mode]["clocks"] = sampler.stop()
             outputs[mode] = [o.sum().item() for _, o in keep[:4]]
     same = outputs["graph"] == outputs["direct"] == outputs["persistent"] == outputs["per_job"]
+    # every compiled backprojection shape (tile, voxels per thread, angles per
+    # chunk) timed alone on the smallest, a middle and the largest job
+    def fbp_ms(j, reps=3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        be.fbp_d(j["sino"], j["depth"], j["num_angles"], j["bins"], j["output_size"], j["filter"], j["out"])
+        e0.record(stream)
+        for _ in range(reps):
+            be.fbp_d(j["sino"], j["depth"], j["num_angles"], j["bins"], j["output_size"], j["filter"], j["out"])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+    order = sorted(range(len(shapes)), key=lambda k: shapes[k]["n"] ** 2 * shapes[k]["nz"] * shapes[k]["na"])
+    shape_times = []
+    for k in (order[0], order[len(order) // 2], order[-1]):
+        row = {"job": shapes[k], "default_shape": be.bp_shape_for(shapes[k]["n"], shapes[k]["nz"], shapes[k]["na"])}
+        for v in range(6):
+            be.set_bp_shape(v)
+            row[f"shape{v}_{'x'.join(str(x) for x in ctb.bp_shape_info(v))}_ms"] = fbp_ms(jobs[k])
+        be.set_bp_shape(-1)
+        shape_times.append(row)
+    # the autotuner: the first job of each size bucket times all shapes on its
+    # own data; the batch then uses the tuned shape of every tuned bucket
+    be.set_autotune(True)
+    for j in jobs:
+        be.fbp_d(j["sino"], j["depth"], j["num_angles"], j["bins"], j["output_size"], j["filter"], j["out"])
+    be.synchronize()
+    table = be.autotune_table()
+    with be.batch(jobs, ctb.BATCH_GRAPH) as b:
+        for _ in range(args.warmup):
+            b.run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_t = e0.elapsed_time(e1) / args.steps
+    be.set_autotune(False)
+    results["graph_autotuned"] = dict(ms_per_step=ms_t, value=updates / (ms_t * 1e-3))
     g = results["graph"]
     line = {
         "metric": METRIC, "value": g["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
@@ -724,6 +766,8 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
         "modes": results,
         "batched_vs_per_job": results["per_job"]["ms_per_step"] / g["ms_per_step"],
         "outputs_identical_across_modes": same,
+        "autotune_table": [dict(zip(("n_bucket", "angle_bucket", "depth_bucket", "shape"), e)) for e in table],
+        "shape_times": shape_times,
         "clocks": g.get("clocks"),
     }
     print(json.dumps(line), flush=True)
