@@ -108,13 +108,10 @@ ctb_status filter_tables(ctb_ctx* ctx, const PadGeom& g, int type, const float2*
     auto key = std::make_pair(g.bins, type + (keep_nyquist ? 16 : 0));
     auto it = ctx->filters.find(key);
     if (it == ctx->filters.end()) {
-        const std::vector<double> Hd = conv_response(g, type, keep_nyquist);
-        std::vector<float2> Hc(Lc);
-        for (int k = 0; k < Lc; ++k)
-            Hc[k] = make_float2(static_cast<float>(Hd[2 * k]), static_cast<float>(Hd[2 * k + 1]));
+        const std::vector<float2> Hc = filter_table(g, type, keep_nyquist);
         DevBuf b;
-        CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float2) * Lc));
-        b.bytes = sizeof(float2) * Lc;
+        CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float2) * Hc.size()));
+        b.bytes = sizeof(float2) * Hc.size();
         CTB_CUDA(ctx, cudaMemcpy(b.ptr, Hc.data(), b.bytes, cudaMemcpyHostToDevice));
         it = ctx->filters.emplace(key, b).first;
     }

@@ -27,8 +27,10 @@ PadGeom pad_geometry(int bins);
 // h = IDFT_L(H~) (H~[k] = H[min(k, L-k)], bins 0 and L/2 zero). Only lags
 // d in [-(pad + bins - 1), sq - 1 - pad] ever meet data, a range of sq + bins - 1
 // <= Lc samples, so the same linear operator is a circular convolution of length
-// Lc with h restricted to those lags. Returns DFT_Lc of that kernel divided by Lc
-// (re, im interleaved), evaluated in double precision.
+// Lc with h restricted to those lags. With the row placed at positions [0, bins)
+// of the length-Lc sequence, lag d sits at (d + pad) mod Lc and filtered bin i
+// is position i. Returns DFT_Lc of that kernel divided by Lc (re, im
+// interleaved), evaluated in double precision.
 std::vector<double> conv_response(const PadGeom& g, int type, bool keep_nyquist = false);
 // The same kernel in the lag domain: h(d) for d = -(pad + bins - 1) .. sq - 1 - pad
 // (index d + pad + bins - 1), double precision. Filtered bin i of a row x is
@@ -117,9 +119,17 @@ cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int
                            cudaStream_t st);
 // Twiddle tables of the filter's FFT of length L (every radix-16 pass and the
 // radix-2/4/8 last pass, r-major per pass), correctly rounded from double
-// precision; fft_twiddle_len(L) entries.
+// precision: fft_twiddle_len(L) float2 entries; for L <= kPackedMaxL followed,
+// from float2 index packed_offset(fft_twiddle_len(L)), by the same entries as
+// float4 {wx, wx, wy, wy} for the packed two-sequence kernel.
+constexpr int kPackedMaxL = 4096;
+inline size_t packed_offset(size_t n) { return (n + 1) & ~size_t(1); }
 size_t fft_twiddle_len(int L);
 std::vector<float2> fft_twiddle_table(int L);
+// The filter's convolution spectrum (conv_response rounded to float2, Lc
+// entries); for Lc <= kPackedMaxL followed by the same values as float4
+// {hx, hx, hy, hy} (Lc of them, from float2 index Lc).
+std::vector<float2> filter_table(const PadGeom& g, int type, bool keep_nyquist = false);
 cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
                           const FiltLayout& fl, const float2* d_Hc, const float2* d_tw,
                           const float4* d_stats, int denorm, float scale, float4* d_filt,
@@ -179,7 +189,7 @@ struct FiltJob {
     float4* filt;         // [nzg][na][pitch]
     const float4* stats;
     const float2* Hc;     // convolution spectrum / Lc
-    int nz, na, bins, sq, pad, guard, pitch, denorm;
+    int nz, na, bins, sq, pad, guard, pitch, denorm;  // pad: pad_before, folded into Hc (rows sit at 0)
     float scale;
     long long first;
 };
@@ -188,6 +198,7 @@ struct FiltBatch {
     int Lc = 0;
     long long total = 0;
     const float2* tw = nullptr;  // fft_twiddle_table(Lc)
+    long long twlen = 0;         // its float2 part (set by launch_filter_batch)
     FiltJob job[kMaxJobs];
 };
 // Conventions of a reconstruction: SerialBackend's (the default, the oracle)

@@ -74,10 +74,13 @@ std::vector<double> conv_kernel(const PadGeom& g, int type, bool keep_nyquist) {
 std::vector<double> conv_response(const PadGeom& g, int type, bool keep_nyquist) {
     const int Lc = g.Lc;
     const std::vector<double> h = conv_kernel(g, type, keep_nyquist);
+    // The device places a row's nd values at positions [0, nd) of the
+    // sequence (not at pad_before), so lag d = i - pad - j is stored at
+    // (d + pad) mod Lc: filtered bin i is then sequence position i.
     std::vector<std::complex<double>> hc(Lc, 0.0);
     const int dmin = -(g.pad + g.bins - 1);
     for (size_t k = 0; k < h.size(); ++k) {
-        const int d = dmin + static_cast<int>(k);
+        const int d = dmin + static_cast<int>(k) + g.pad;
         hc[((d % Lc) + Lc) % Lc] = h[k];
     }
     fft64(hc);

@@ -36,10 +36,16 @@ constexpr size_t kOffErr = 0;
 constexpr size_t kOffAngles = 256;
 constexpr size_t kOffTrig = kOffAngles + sizeof(float) * kMaxAngles;           // double2 + float2
 constexpr size_t kOffHc = kOffTrig + (sizeof(double2) + sizeof(float2)) * kMaxAngles;
-constexpr size_t kOffTw = kOffHc + sizeof(float2) * kMaxConv;
-// FFT twiddle tables of the longest convolution (fft_twiddle_len(8192) =
-// 15 (8192/8 - 1) + 1 x 4096 entries), rounded up to 256 bytes
-constexpr size_t kTwEntries = 15 * (kMaxConv / 8 - 1) + kMaxConv / 2;
+// The filter spectrum (filter_table): Lc float2, plus Lc packed float4 when
+// Lc <= 4096, so at most max(8192, 3 x 4096) float2.
+constexpr size_t kHcEntries = 3 * kMaxConv / 2;
+constexpr size_t kOffTw = kOffHc + sizeof(float2) * kHcEntries;
+// FFT twiddle tables (fft_twiddle_table): the longest is the one of Lc = 4096
+// with its packed copy, 15 (4096/8 - 1) = 7665 float2, one float2 of
+// alignment, then 7665 float4; Lc = 8192 has 15 (8192/8 - 1) + 4096 = 19441
+// float2. Rounded up to 256 bytes.
+constexpr size_t kTwEntries = 3 * (15 * (4096 / 8 - 1)) + 1;
+static_assert(kTwEntries >= 15 * (kMaxConv / 8 - 1) + kMaxConv / 2, "twiddle region too small");
 constexpr size_t kOffFilt = kOffTw + (sizeof(float2) * kTwEntries + 255) / 256 * 256;
 constexpr size_t kFiltCapacity = (kScratchBytes - kOffFilt) / sizeof(float4);  // float4 bins
 static_assert(kOffTrig % 256 == 0 && kOffHc % 256 == 0 && kOffTw % 256 == 0 && kOffFilt % 256 == 0,
@@ -102,12 +108,9 @@ extern "C" ctb_status ctb_fbp_noalloc(const float* d_sino, int depth, int num_an
         const float th = deg[a] * 3.14159265358979323846f / 180.0f;
         csf[a] = make_float2(std::cos(th), std::sin(th));
     }
-    const std::vector<double> Hd = conv_response(g, filter);
-    std::vector<float2> Hc(g.Lc);
-    for (int k = 0; k < g.Lc; ++k)
-        Hc[k] = make_float2(static_cast<float>(Hd[2 * k]), static_cast<float>(Hd[2 * k + 1]));
+    const std::vector<float2> Hc = filter_table(g, filter);
     const std::vector<float2> tw = fft_twiddle_table(g.Lc);
-    if (tw.size() > kTwEntries) return CTB_ERR_UNSUPPORTED;
+    if (Hc.size() > kHcEntries || tw.size() > kTwEntries) return CTB_ERR_UNSUPPORTED;
     unsigned* d_err = reinterpret_cast<unsigned*>(base + kOffErr);
     float* d_deg = reinterpret_cast<float*>(base + kOffAngles);
     double2* d_cs = reinterpret_cast<double2*>(base + kOffTrig);
@@ -119,7 +122,7 @@ extern "C" ctb_status ctb_fbp_noalloc(const float* d_sino, int depth, int num_an
     cudaError_t e = cudaMemsetAsync(d_err, 0, sizeof(unsigned), st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_deg, deg.data(), sizeof(float) * num_angles, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_csf, csf.data(), sizeof(float2) * num_angles, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_Hc, Hc.data(), sizeof(float2) * g.Lc, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_Hc, Hc.data(), sizeof(float2) * Hc.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = launch_trig(d_deg, num_angles, d_cs, st);
     const float scale = 3.14159265358979323846f / (2.0f * static_cast<float>(num_angles));

@@ -22,12 +22,13 @@ namespace ctb {
 namespace {
 
 constexpr int TX = 32, TY = 8, TZ = 4;  // CTA tile: 32 x 8 x 4 voxels, 256 threads
+constexpr int TZS = 8;                  // k_phantom_sum: 32 x 8 x 8 voxels, 8 slices per thread
 constexpr int MAXC = 1024;              // candidate list capacity per CTA
 
 // Ordered compaction of the ellipsoids whose box meets the tile.
 // boxes: 6 ints per ellipsoid {x0, x1, y0, y1, z0, z1} (inclusive).
 __device__ int cull(const int* __restrict__ boxes, int k, int x0, int y0, int z0,
-                    short* cand, int* warp_tot) {
+                    short* cand, int* warp_tot, int tz = TZ) {
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     int total = 0;
     for (int base = 0; base < k; base += blockDim.x) {
@@ -36,7 +37,7 @@ __device__ int cull(const int* __restrict__ boxes, int k, int x0, int y0, int z0
         if (e < k) {
             const int* b = boxes + 6 * e;
             hit = !(b[1] < x0 || b[0] > x0 + TX - 1 || b[3] < y0 || b[2] > y0 + TY - 1 ||
-                    b[5] < z0 || b[4] > z0 + TZ - 1);
+                    b[5] < z0 || b[4] > z0 + tz - 1);
         }
         const unsigned m = __ballot_sync(0xffffffffu, hit);
         if (lane == 0) warp_tot[wid] = __popc(m);
@@ -60,56 +61,114 @@ __device__ __forceinline__ float grid_coord(int i, int n) {
                      static_cast<float>(n));
 }
 
+// One ellipsoid staged for k_phantom_sum: the coefficients of the terms in x
+// and y (the same for a thread's 8 slices) as scalars, those that meet the
+// slice coordinate as duplicated pairs for the packed FP32x2 instructions.
+struct PhEll {
+    float cx, cy, r00, r01, r10, r11, r20, r21;         // p0 p1 p3 p4 p6 p7 p9 p10
+    float2 cz, r02, r12, r22, i0, i1, i2, dens;          // p2 p5 p8 p11 p12 p13 p14 p15, each twice
+};
+
+// a - b as one packed instruction: fma(b, -1, a) rounds a - b exactly once
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+
+// Every thread holds one (x, y) column of TZS slices; the slice terms run two
+// slices per packed FP32x2 instruction. Each lane of a packed add or multiply
+// is the IEEE round-to-nearest result of the scalar operation, in the same
+// order as the scalar code of the oracle, so the phantom stays bit-identical.
 __global__ void __launch_bounds__(256) k_phantom_sum(const float* __restrict__ params,
                                                      const int* __restrict__ boxes, int k, int nx,
                                                      int ny, int nz, float* __restrict__ vol) {
     __shared__ short cand[MAXC];
     __shared__ int warp_tot[8];
-    __shared__ float sp[64][16];
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
-    const int nc = cull(boxes, k, x0, y0, z0, cand, warp_tot);
+    __shared__ PhEll sp[64];
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZS;
+    // A tile whose voxel nearest the centre lies outside the unit sphere holds
+    // only zeros: the rounded r^2 below grows with every |coordinate|, so no
+    // voxel of the tile passes r2 <= 1 (the test is the voxels' own expression
+    // on coordinates no larger than theirs). Such tiles skip the ellipsoids.
+    const bool outside = [&] {
+        auto nearest = [](int lo, int len, int n) {
+            const int hi = min(lo + len, n) - 1;
+            if (2 * hi < n - 1) return fabsf(grid_coord(hi, n));
+            if (2 * lo > n - 1) return fabsf(grid_coord(lo, n));
+            return 0.0f;  // the tile straddles the centre plane
+        };
+        const float mx = nearest(x0, TX, nx), my = nearest(y0, TY, ny), mz = nearest(z0, TZS, nz);
+        return __fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)) > 1.0f;
+    }();
+    const int nc = outside ? 0 : cull(boxes, k, x0, y0, z0, cand, warp_tot, TZS);
     const bool overflow = nc > MAXC;  // fall back to every ellipsoid
     const int ncand = overflow ? k : nc;
     const int x = x0 + (threadIdx.x & 31), y = y0 + (threadIdx.x >> 5);
     const bool live_xy = x < nx && y < ny;
     const float X = grid_coord(x, nx), Y = grid_coord(y, ny);
-    float acc[TZ];
-    float Z[TZ];
-    bool in[TZ];
+    constexpr int NPAIR = TZS / 2;
+    float acc[TZS];
+    float2 Z[NPAIR];
+    bool in[TZS];
 #pragma unroll
-    for (int j = 0; j < TZ; ++j) {
+    for (int j = 0; j < TZS; ++j) {
         acc[j] = 0.0f;
-        Z[j] = grid_coord(z0 + j, nz);
-        const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(X, X), __fmul_rn(Y, Y)), __fmul_rn(Z[j], Z[j]));
+        const float zj = grid_coord(z0 + j, nz);
+        if (j & 1) Z[j / 2].y = zj;
+        else Z[j / 2].x = zj;
+        const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(X, X), __fmul_rn(Y, Y)), __fmul_rn(zj, zj));
         in[j] = r2 <= 1.0f;
     }
     for (int base = 0; base < ncand; base += 64) {
         const int cnt = min(64, ncand - base);
         __syncthreads();
-        for (int i = threadIdx.x; i < cnt * 16; i += blockDim.x) {
-            const int e = overflow ? base + i / 16 : cand[base + i / 16];
-            sp[i / 16][i % 16] = params[16 * e + (i % 16)];
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+            const int e = overflow ? base + i : cand[base + i];
+            const float* p = params + 16 * e;
+            PhEll q;
+            q.cx = p[0];
+            q.cy = p[1];
+            q.r00 = p[3];
+            q.r01 = p[4];
+            q.r10 = p[6];
+            q.r11 = p[7];
+            q.r20 = p[9];
+            q.r21 = p[10];
+            q.cz = make_float2(p[2], p[2]);
+            q.r02 = make_float2(p[5], p[5]);
+            q.r12 = make_float2(p[8], p[8]);
+            q.r22 = make_float2(p[11], p[11]);
+            q.i0 = make_float2(p[12], p[12]);
+            q.i1 = make_float2(p[13], p[13]);
+            q.i2 = make_float2(p[14], p[14]);
+            q.dens = make_float2(p[15], p[15]);
+            sp[i] = q;
         }
         __syncthreads();
         for (int c = 0; c < cnt; ++c) {
-            const float* p = sp[c];
-            const float dx = __fsub_rn(X, p[0]), dy = __fsub_rn(Y, p[1]);
+            const PhEll& q = sp[c];
+            const float dx = __fsub_rn(X, q.cx), dy = __fsub_rn(Y, q.cy);
+            // the x and y terms of the three body coordinates, shared by the slices
+            const float u0 = __fadd_rn(__fmul_rn(q.r00, dx), __fmul_rn(q.r01, dy));
+            const float u1 = __fadd_rn(__fmul_rn(q.r10, dx), __fmul_rn(q.r11, dy));
+            const float u2 = __fadd_rn(__fmul_rn(q.r20, dx), __fmul_rn(q.r21, dy));
+            const float2 U0 = make_float2(u0, u0), U1 = make_float2(u1, u1), U2 = make_float2(u2, u2);
 #pragma unroll
-            for (int j = 0; j < TZ; ++j) {
-                const float dz = __fsub_rn(Z[j], p[2]);
-                const float b0 = __fadd_rn(__fadd_rn(__fmul_rn(p[3], dx), __fmul_rn(p[4], dy)), __fmul_rn(p[5], dz));
-                const float b1 = __fadd_rn(__fadd_rn(__fmul_rn(p[6], dx), __fmul_rn(p[7], dy)), __fmul_rn(p[8], dz));
-                const float b2 = __fadd_rn(__fadd_rn(__fmul_rn(p[9], dx), __fmul_rn(p[10], dy)), __fmul_rn(p[11], dz));
-                const float q = __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(b0, b0), p[12]),
-                                                    __fmul_rn(__fmul_rn(b1, b1), p[13])),
-                                          __fmul_rn(__fmul_rn(b2, b2), p[14]));
-                if (in[j] && q <= 1.0f) acc[j] = __fadd_rn(acc[j], p[15]);
+            for (int h = 0; h < NPAIR; ++h) {
+                const float2 dz = sub2(Z[h], q.cz);
+                const float2 b0 = __fadd2_rn(U0, __fmul2_rn(q.r02, dz));
+                const float2 b1 = __fadd2_rn(U1, __fmul2_rn(q.r12, dz));
+                const float2 b2 = __fadd2_rn(U2, __fmul2_rn(q.r22, dz));
+                const float2 qq = __fadd2_rn(__fadd2_rn(__fmul2_rn(__fmul2_rn(b0, b0), q.i0),
+                                                        __fmul2_rn(__fmul2_rn(b1, b1), q.i1)),
+                                             __fmul2_rn(__fmul2_rn(b2, b2), q.i2));
+                if (in[2 * h] && qq.x <= 1.0f) acc[2 * h] = __fadd_rn(acc[2 * h], q.dens.x);
+                if (in[2 * h + 1] && qq.y <= 1.0f) acc[2 * h + 1] = __fadd_rn(acc[2 * h + 1], q.dens.y);
             }
         }
     }
     if (!live_xy) return;
 #pragma unroll
-    for (int j = 0; j < TZ; ++j) {
+    for (int j = 0; j < TZS; ++j) {
         const int z = z0 + j;
         if (z < nz) vol[(static_cast<long long>(z) * ny + y) * nx + x] = acc[j];
     }
@@ -215,7 +274,7 @@ __global__ void __launch_bounds__(PC_THREADS) k_point_write(
 
 cudaError_t launch_phantom_sum_boxes(const float* d_params, const int* d_boxes, int k, int nx,
                                      int ny, int nz, float* d_vol, cudaStream_t st) {
-    const dim3 grid((nx + TX - 1) / TX, (ny + TY - 1) / TY, (nz + TZ - 1) / TZ);
+    const dim3 grid((nx + TX - 1) / TX, (ny + TY - 1) / TY, (nz + TZS - 1) / TZS);
     k_phantom_sum<<<grid, 256, 0, st>>>(d_params, d_boxes, k, nx, ny, nz, d_vol);
     return cudaGetLastError();
 }

@@ -253,13 +253,10 @@ ctb_status request_tables(ctb_server* s, SReq* q) {
     auto key = std::make_pair(q->r.bins, q->r.filter);
     auto it = s->filters.find(key);
     if (it == s->filters.end()) {
-        const std::vector<double> Hd = conv_response(q->g, q->r.filter);
-        std::vector<float2> Hc(Lc);
-        for (int k = 0; k < Lc; ++k)
-            Hc[k] = make_float2(static_cast<float>(Hd[2 * k]), static_cast<float>(Hd[2 * k + 1]));
+        const std::vector<float2> Hc = filter_table(q->g, q->r.filter);
         DevBuf b;
-        if (cudaMalloc(&b.ptr, sizeof(float2) * Lc) != cudaSuccess) return CTB_ERR_OOM;
-        b.bytes = sizeof(float2) * Lc;
+        if (cudaMalloc(&b.ptr, sizeof(float2) * Hc.size()) != cudaSuccess) return CTB_ERR_OOM;
+        b.bytes = sizeof(float2) * Hc.size();
         if (cudaMemcpyAsync(b.ptr, Hc.data(), b.bytes, cudaMemcpyHostToDevice, s->table_stream) != cudaSuccess ||
             cudaStreamSynchronize(s->table_stream) != cudaSuccess) {
             cudaFree(b.ptr);

@@ -114,10 +114,11 @@ def test_nonuniform_angles(backend):
 
 
 @pytest.mark.parametrize("n,na,nd", [(33, 50, 47), (100, 37, 141), (65, 2100, 93), (20, 16, 11),
-                                     (128, 180, 183)])
+                                     (128, 180, 183), (256, 90, 363), (1768, 24, 2501)])
 def test_reconstruct_slice_shapes(backend, n, na, nd):
     # odd sizes, sizes off the 32-voxel tile grid, > 2048 angles, detector
-    # narrower than the image (taps outside the detector are skipped)
+    # narrower than the image (taps outside the detector are skipped), and
+    # convolution lengths 64 ... 8192 (the last one the scalar FFT kernel)
     rng = np.random.default_rng(n * 1000 + na)
     sl = ellipse_slice(rng, n, 4)
     s32, ang, _ = O.sinogram_f32(sl, na, nd)
@@ -269,7 +270,7 @@ def test_from_sinograms(backend, golden, denorm):
 
 
 # ----------------------------------------------------------------- phantoms
-@pytest.mark.parametrize("shape", [(16, 16, 16), (33, 20, 7), (64, 64, 48)])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (33, 20, 7), (64, 64, 48), (128, 96, 120)])
 def test_phantom_sum_bit_exact(backend, shape):
     nx, ny, nz = shape
     p = ctb.phantom_params(42, 24)
