@@ -146,6 +146,24 @@ def accuracy_report(vol_host, outputs: dict, na: int, nd: int, kind: int, zs):
     return rep
 
 
+def fft_fp32_roofline(nd: int, sq: int, nz: int, na: int, ms: float):
+    """The filter's arithmetic against the FP32 pipe: the nominal 5 L log2 L
+    flops of a complex FFT of the convolution length L = nextPow2(sq + nd - 1),
+    a forward and an inverse transform plus the 6 L of the spectrum product per
+    pair of rows (two real rows travel as one complex sequence), against
+    148 SMs x 128 lanes x 2 flops x 1.965 GHz (the B200's FP32 FMA peak at its
+    maximum clock; packed FP32x2 instructions do not raise it)."""
+    L = 64
+    while L < sq + nd - 1:
+        L *= 2
+    flops = ((nz + 1) // 2) * na * (2 * 5 * L * math.log2(L) + 6 * L)
+    peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    achieved = flops / (ms * 1e-3) / 1e12
+    return {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "algorithmic": f"nominal FFT flops: 2 x 5 L log2 L + 6 L per row pair, L = {L}",
+            "peak_source": "nominal FP32 FMA peak of a B200 at 1965 MHz (148 SMs)"}
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
@@ -405,6 +423,12 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
     vol = torch.empty((nz, n, n), dtype=torch.float32, device="cuda")
     out = torch.empty_like(vol)
     be.phantom_d(params, n, n, nz, vol.data_ptr())
+    # the phantom kernel's own device time (events around its launch), after a warm-up
+    phantom_ms = []
+    for _ in range(3):
+        be.phantom_d(params, n, n, nz, out.data_ptr())
+        phantom_ms.append(be.last_phantom_ms())
+    phantom_ms = statistics.median(phantom_ms)
 
     def step():
         be.reconstruct_volume_d(vol.data_ptr(), n, nz, na, nd, kind, out.data_ptr())
@@ -527,11 +551,20 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
                          "note": "filter + backprojection kernels only"},
             "roofline": roof_main,
             "roofline_" + roof_other["kernel"][2:]: roof_other,
+            "roofline_phantom": {"kernel": "k_phantom_sum", "bound": "hbm",
+                                 "achieved": 4.0 * n * n * nz / (phantom_ms * 1e-3) / 1e9, "peak": hbm_peak,
+                                 "unit": "GB/s",
+                                 "frac": (4.0 * n * n * nz / (phantom_ms * 1e-3) / 1e9 / hbm_peak) if hbm_peak else None,
+                                 "ms": phantom_ms, "ellipsoids": cfg["ellipsoids"],
+                                 "algorithmic": "4 B written per voxel (N^3 float32)",
+                                 "peak_source": "hbm_gbs, " + peaks["_label"] if hbm_peak else None},
             "roofline_filter": {"kernel": "k_filter", "bound": "hbm",
                                 "achieved": filt_bytes / (filt_kernel_ms * 1e-3) / 1e9,
                                 "peak": hbm_peak, "unit": "GB/s",
                                 "frac": (filt_bytes / (filt_kernel_ms * 1e-3) / 1e9 / hbm_peak) if hbm_peak else None,
-                                "peak_source": "hbm_gbs, " + peaks["_label"] if hbm_peak else None},
+                                "peak_source": "hbm_gbs, " + peaks["_label"] if hbm_peak else None,
+                                "ms": filt_kernel_ms,
+                                "fp32": fft_fp32_roofline(nd, sq, nz, na, filt_kernel_ms)},
             "e2e": {"value": replica_throughput(world, updates, e2e_ms), "unit": UNIT,
                     "h2d_bytes_per_step": 4 * n * n * nz, "d2h_bytes_per_step": 4 * n * n * nz,
                     "ms_per_step": e2e_ms, "api": "ctb_reconstruct_volume (pinned host buffers)"},

@@ -89,6 +89,9 @@ ctb_status ctb_synchronize(ctb_ctx* ctx);
  * filter+backprojection stages, measured with CUDA events. */
 double ctb_last_sinogram_ms(const ctb_ctx* ctx);
 double ctb_last_reconstruction_ms(const ctb_ctx* ctx);
+/* Device time of the last summed-ellipsoid phantom kernel (ctb_phantom_sum[_d]),
+ * CUDA events around its launch; no counterpart in the reference. */
+double ctb_last_phantom_ms(const ctb_ctx* ctx);
 /* Number of kernel launches the context has issued so far. */
 uint64_t ctb_launch_count(const ctb_ctx* ctx);
 

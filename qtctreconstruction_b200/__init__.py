@@ -143,6 +143,8 @@ def _declare(L):
     L.ctb_last_sinogram_ms.restype = ctypes.c_double
     L.ctb_last_reconstruction_ms.argtypes = [p]
     L.ctb_last_reconstruction_ms.restype = ctypes.c_double
+    L.ctb_last_phantom_ms.argtypes = [p]
+    L.ctb_last_phantom_ms.restype = ctypes.c_double
     L.ctb_launch_count.argtypes = [p]
     L.ctb_launch_count.restype = u64
     L.ctb_pad_geometry.argtypes = [i, P(i), P(i), P(i)]
@@ -438,6 +440,10 @@ class B200Backend:
 
     def lastSinogramTimeMs(self) -> float:
         return float(self._lib.ctb_last_sinogram_ms(self._h))
+
+    def last_phantom_ms(self) -> float:
+        """Device time of the last summed-ellipsoid phantom kernel."""
+        return float(self._lib.ctb_last_phantom_ms(self._h))
 
     def lastReconstructionTimeMs(self) -> float:
         return float(self._lib.ctb_last_reconstruction_ms(self._h))

@@ -611,6 +611,7 @@ ctb_status ctb_synchronize(ctb_ctx* ctx) {
 
 double ctb_last_sinogram_ms(const ctb_ctx* ctx) { return ctx ? ctx->last_sino_ms : 0.0; }
 double ctb_last_reconstruction_ms(const ctb_ctx* ctx) { return ctx ? ctx->last_recon_ms : 0.0; }
+double ctb_last_phantom_ms(const ctb_ctx* ctx) { return ctx ? ctx->last_phantom_ms : 0.0; }
 uint64_t ctb_launch_count(const ctb_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 ctb_status ctb_pad_geometry(int bins, int* square_bins, int* pad_before, int* fft_size) {
@@ -1071,9 +1072,14 @@ ctb_status ctb_phantom_sum_d(ctb_ctx* ctx, const float* params, int count, int n
         CTB_CUDA(ctx, cudaMemcpyAsync(d_p, params, sizeof(float) * 16 * count, cudaMemcpyHostToDevice, ctx->stream));
         CTB_CUDA(ctx, cudaMemcpyAsync(d_b, boxes.data(), sizeof(int) * 6 * count, cudaMemcpyHostToDevice, ctx->stream));
     }
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
     CTB_LAUNCH(ctx, launch_phantom_sum_boxes(d_p, d_b, count, nx, ny, nz, d_vol, ctx->stream));
+    CTB_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
     // the host vectors must outlive the asynchronous copies
     CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+    ctx->last_phantom_ms = ms;
     return CTB_OK;
 }
 

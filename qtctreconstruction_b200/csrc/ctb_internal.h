@@ -122,7 +122,7 @@ cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int
 // precision: fft_twiddle_len(L) float2 entries; for L <= kPackedMaxL followed,
 // from float2 index packed_offset(fft_twiddle_len(L)), by the same entries as
 // float4 {wx, wx, wy, wy} for the packed two-sequence kernel.
-constexpr int kPackedMaxL = 4096;
+constexpr int kPackedMaxL = 2048;
 inline size_t packed_offset(size_t n) { return (n + 1) & ~size_t(1); }
 size_t fft_twiddle_len(int L);
 std::vector<float2> fft_twiddle_table(int L);
@@ -245,6 +245,7 @@ struct ctb_ctx {
     uint64_t launches = 0;
     double last_sino_ms = 0.0;
     double last_recon_ms = 0.0;
+    double last_phantom_ms = 0.0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // Copy streams and per-slab events of the host-buffer volume pipeline
     // (created on first use).

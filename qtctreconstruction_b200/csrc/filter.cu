@@ -574,7 +574,7 @@ __device__ __forceinline__ void dftp(C2* v) {
 // Shared-memory element p (a float4: one C2) lives at p ^ f(p >> 3),
 // f(q) = (q + q / 8) mod 8: a permutation inside every group of 8 elements
 // that keeps the 8 lanes of each LDS.128/STS.128 phase on distinct banks for
-// the unit, 8 and 16 strides of the passes at every length from 64 to 4096
+// the unit, 8 and 16 strides of the passes at every length from 64 to 2048
 // except one pass at 512 and 1024 (two-way).
 __device__ __forceinline__ int swz(int p) { return p ^ (((p >> 3) + (p >> 6)) & 7); }
 __device__ __forceinline__ C2 ld_c2(const float4* buf, int p) {
@@ -620,12 +620,13 @@ __device__ __forceinline__ void passes16p(float4* buf, int j, const float4* __re
     }
 }
 
-// Up to length 2048 the registers are held to 128 (four CTAs per SM, no
-// spills); at 4096 a 128-register cap spills, so the kernel keeps its own
-// allocation (one 256-thread CTA per SM).
+// Lengths up to kPackedMaxL = 2048. The registers are held to 96 (five CTAs
+// per SM at 2048, a few spilled bytes); the kernel is latency-bound, so the
+// extra warps pay. At 4096 the 16 pairs per thread would need more than 128
+// registers (one 256-thread CTA per SM), slower than the scalar kernel, which
+// therefore keeps lengths 4096 and 8192.
 template <int LOGL>
-__global__ void __launch_bounds__((1 << LOGL) / 16, LOGL >= 12 ? 1 : 4)
-    k_filter4(const __grid_constant__ FiltBatch batch) {
+__global__ void __launch_bounds__((1 << LOGL) / 16, 5) k_filter4(const __grid_constant__ FiltBatch batch) {
     constexpr int L = 1 << LOGL, T = L / 16, REM = LOGL & 3, Q = LOGL >> 2;
     constexpr int R0 = REM ? (1 << REM) : 16;  // radix of the first and the last pass
     constexpr int NB0 = 16 / R0;               // their butterflies per thread
@@ -818,6 +819,9 @@ cudaError_t launch_filter4(const FiltBatch& b, cudaStream_t st) {
     const size_t smem = sizeof(float4) * L;
     cudaError_t e = cudaFuncSetAttribute(k_filter4<LOGL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
+    // all of the unified L1 / shared storage as shared memory: five 32 KB CTAs per SM at 2048
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_filter4<LOGL>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
     const long long gx = b.total < 65535 ? b.total : 65535;
     const long long gy = (b.total + gx - 1) / gx;
@@ -840,14 +844,14 @@ cudaError_t launch_filter_batch(const FiltBatch& b, cudaStream_t st) {
             p.job[k].first = p.total;
             p.total += static_cast<long long>(p.job[k].na) * ((p.job[k].nz + 3) / 4);
         }
+        static_assert(kPackedMaxL == 2048, "one instantiation per length up to kPackedMaxL");
         switch (logL) {
         case 6: return launch_filter4<6>(p, st);
         case 7: return launch_filter4<7>(p, st);
         case 8: return launch_filter4<8>(p, st);
         case 9: return launch_filter4<9>(p, st);
         case 10: return launch_filter4<10>(p, st);
-        case 11: return launch_filter4<11>(p, st);
-        default: return launch_filter4<12>(p, st);
+        default: return launch_filter4<11>(p, st);
         }
     }
     const int K = L > 4096 ? 2 : 1;

@@ -37,15 +37,15 @@ constexpr size_t kOffAngles = 256;
 constexpr size_t kOffTrig = kOffAngles + sizeof(float) * kMaxAngles;           // double2 + float2
 constexpr size_t kOffHc = kOffTrig + (sizeof(double2) + sizeof(float2)) * kMaxAngles;
 // The filter spectrum (filter_table): Lc float2, plus Lc packed float4 when
-// Lc <= 4096, so at most max(8192, 3 x 4096) float2.
-constexpr size_t kHcEntries = 3 * kMaxConv / 2;
+// Lc <= 2048, so at most max(8192, 3 x 2048) = 8192 float2.
+constexpr size_t kHcEntries = kMaxConv;
+static_assert(3 * 2048 <= kHcEntries, "spectrum region too small");
 constexpr size_t kOffTw = kOffHc + sizeof(float2) * kHcEntries;
-// FFT twiddle tables (fft_twiddle_table): the longest is the one of Lc = 4096
-// with its packed copy, 15 (4096/8 - 1) = 7665 float2, one float2 of
-// alignment, then 7665 float4; Lc = 8192 has 15 (8192/8 - 1) + 4096 = 19441
-// float2. Rounded up to 256 bytes.
-constexpr size_t kTwEntries = 3 * (15 * (4096 / 8 - 1)) + 1;
-static_assert(kTwEntries >= 15 * (kMaxConv / 8 - 1) + kMaxConv / 2, "twiddle region too small");
+// FFT twiddle tables (fft_twiddle_table): the longest is that of Lc = 8192,
+// 15 (8192/8 - 1) + 4096 = 19441 float2 (Lc = 2048 with its packed copy takes
+// 3 x 5617 + 1). Rounded up to 256 bytes.
+constexpr size_t kTwEntries = 15 * (kMaxConv / 8 - 1) + kMaxConv / 2;
+static_assert(3 * (15 * (2048 / 8 - 1) + 7 * (2048 / 8)) + 1 <= kTwEntries, "twiddle region too small");
 constexpr size_t kOffFilt = kOffTw + (sizeof(float2) * kTwEntries + 255) / 256 * 256;
 constexpr size_t kFiltCapacity = (kScratchBytes - kOffFilt) / sizeof(float4);  // float4 bins
 static_assert(kOffTrig % 256 == 0 && kOffHc % 256 == 0 && kOffTw % 256 == 0 && kOffFilt % 256 == 0,

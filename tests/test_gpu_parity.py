@@ -119,12 +119,20 @@ def test_reconstruct_slice_shapes(backend, n, na, nd):
     # odd sizes, sizes off the 32-voxel tile grid, > 2048 angles, detector
     # narrower than the image (taps outside the detector are skipped), and
     # convolution lengths 64 ... 8192 (the last one the scalar FFT kernel)
+    # (at n = 1768 SerialBackend's own float result is 1.5e-4 from the FP64
+    # rerun, so there the gate is the FP64 rerun, which the GPU must also meet
+    # at least as well as SerialBackend does)
     rng = np.random.default_rng(n * 1000 + na)
     sl = ellipse_slice(rng, n, 4)
     s32, ang, _ = O.sinogram_f32(sl, na, nd)
     ser = O.reconstruct_slice_f32(s32, ang, n, O.SHEPP_LOGAN)
     gpu = backend.reconstructSlice(ctb.Sinogram(s32, ang), n, ReconstructionParams(FilterType.SheppLogan, na))
-    _close(gpu, ser)
+    if n <= 256:
+        _close(gpu, ser)
+    else:
+        f64 = O.reconstruct_slice_f64(s32.astype(np.float64), ang, n, O.SHEPP_LOGAN)
+        _close(gpu, f64)
+        assert O.rel_l2(gpu, f64) <= O.rel_l2(ser, f64)
 
 
 def test_output_size_larger_than_detector(backend):

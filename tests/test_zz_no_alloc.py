@@ -33,12 +33,12 @@ MAX_ABS = 1e-4
 
 # The static array: 16 MiB, of which the filtered rows get what the fixed
 # tables leave, in float4 bins: the error word (256 B), 2048 angles of degrees
-# (4 B) and trig (24 B), the filter spectrum (at most 3 x 4096 float2: 4096
-# values and their packed copy) and the FFT twiddle tables (at most those of
-# length 4096 with their packed copy, 3 x 7665 + 1 float2, rounded up to 256 B).
-_HC_BYTES = 8 * 3 * 8192 // 2
-_TW_BYTES = (8 * (3 * 15 * (4096 // 8 - 1) + 1) + 255) // 256 * 256
-FILT_CAPACITY = ((16 << 20) - (256 + 4 * 2048 + 24 * 2048 + _HC_BYTES + _TW_BYTES)) // 16
+# (4 B) and trig (24 B), the spectrum of an 8192-long convolution (8 B each)
+# and the FFT twiddle tables of that length (15 (8192/8 - 1) + 4096 complex
+# values, rounded up to 256 B); the packed copies the shorter lengths add fit
+# in the same room.
+_TW_BYTES = (8 * (15 * (8192 // 8 - 1) + 8192 // 2) + 255) // 256 * 256
+FILT_CAPACITY = ((16 << 20) - (256 + 4 * 2048 + 24 * 2048 + 8 * 8192 + _TW_BYTES)) // 16
 
 
 def _pitch(bins, n_out):
