@@ -620,13 +620,14 @@ __device__ __forceinline__ void passes16p(float4* buf, int j, const float4* __re
     }
 }
 
-// Lengths up to kPackedMaxL = 2048. The registers are held to 96 (five CTAs
-// per SM at 2048, a few spilled bytes); the kernel is latency-bound, so the
-// extra warps pay. At 4096 the 16 pairs per thread would need more than 128
-// registers (one 256-thread CTA per SM), slower than the scalar kernel, which
-// therefore keeps lengths 4096 and 8192.
+// Lengths up to kPackedMaxL = 2048, registers held to 128 (four CTAs per SM
+// at 2048, no spills; a 96-register cap for a fifth CTA spills and measured
+// slower, 1.81 against 1.56 ms at 512^3 x 720). At 4096 the 16 pairs per
+// thread need more than 128 registers (one 256-thread CTA per SM) and the
+// kernel is slower than the scalar one (5.35 against 4.68 ms at 1024^2 x 256 x
+// 1440), which therefore keeps lengths 4096 and 8192.
 template <int LOGL>
-__global__ void __launch_bounds__((1 << LOGL) / 16, 5) k_filter4(const __grid_constant__ FiltBatch batch) {
+__global__ void __launch_bounds__((1 << LOGL) / 16, 4) k_filter4(const __grid_constant__ FiltBatch batch) {
     constexpr int L = 1 << LOGL, T = L / 16, REM = LOGL & 3, Q = LOGL >> 2;
     constexpr int R0 = REM ? (1 << REM) : 16;  // radix of the first and the last pass
     constexpr int NB0 = 16 / R0;               // their butterflies per thread
@@ -819,7 +820,7 @@ cudaError_t launch_filter4(const FiltBatch& b, cudaStream_t st) {
     const size_t smem = sizeof(float4) * L;
     cudaError_t e = cudaFuncSetAttribute(k_filter4<LOGL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
-    // all of the unified L1 / shared storage as shared memory: five 32 KB CTAs per SM at 2048
+    // prefer shared memory in the unified L1 / shared storage (32 KB per CTA at 2048)
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_filter4<LOGL>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
