@@ -761,7 +761,7 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
     shape_times = []
     for k in (order[0], order[len(order) // 2], order[-1]):
         row = {"job": shapes[k], "default_shape": be.bp_shape_for(shapes[k]["n"], shapes[k]["nz"], shapes[k]["na"])}
-        for v in range(7):
+        for v in range(6):
             be.set_bp_shape(v)
             row[f"shape{v}_{'x'.join(str(x) for x in ctb.bp_shape_info(v))}_ms"] = fbp_ms(jobs[k])
         be.set_bp_shape(-1)

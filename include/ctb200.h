@@ -117,15 +117,12 @@ ctb_status ctb_filter_kernel_ms(ctb_ctx* ctx, int back, double* ms);
 enum { CTB_FILTER_MODE_FFT = 0, CTB_FILTER_MODE_TC_BF16X3 = 1 };
 ctb_status ctb_set_filter_mode(ctb_ctx* ctx, int mode);
 
-/* Backprojection tile shapes. Seven are compiled: 0 = 32x32 voxels, 4 per
+/* Backprojection tile shapes. Six are compiled: 0 = 32x32 voxels, 4 per
  * thread (the general case); 1 = 64x32, 8 per thread; 2 = 32x16, 2 per
- * thread; 3 = 16x16, 1 per thread; all with 32 angles per staged chunk; the
- * 32x32 tile with 16 (4) and 64 (5) angles per chunk, which sum every
+ * thread; 3 = 16x16, 1 per thread; all with 32 angles per staged chunk; and
+ * the 32x32 tile with 16 (4) and 64 (5) angles per chunk, which sum every
  * voxel's angles in the same order as shape 0 and so give its result bit for
- * bit; and 6 = the 32x32 tile with each thread's 4 voxels a column along y,
- * walked in increasing detector coordinate so that neighbouring voxels share
- * filtered-row taps (same results up to rounding).
- * Without tuning a job gets a shape from its size alone (32x32 once its
+ * bit. Without tuning a job gets a shape from its size alone (32x32 once its
  * tiles x slice groups reach the SM count, 32x16 above a quarter of it, else
  * 16x16). With the autotuner
  * on, the first job of each size bucket {ceil(n / 64), ceil(angles / 180),

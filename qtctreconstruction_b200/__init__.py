@@ -512,7 +512,7 @@ class B200Backend:
         self._check(self._lib.ctb_set_filter_mode(self._h, int(mode)), "set_filter_mode")
 
     def set_bp_shape(self, variant: int):
-        """Force a backprojection tile shape (0..6, see bp_shape_info); -1 = automatic."""
+        """Force a backprojection tile shape (0..5, see bp_shape_info); -1 = automatic."""
         self._check(self._lib.ctb_set_bp_shape(self._h, int(variant)), "set_bp_shape")
 
     def bp_shape_for(self, output_size: int, depth: int, num_angles: int) -> int:

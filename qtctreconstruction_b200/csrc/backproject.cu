@@ -47,20 +47,11 @@ constexpr int kRoundBits = 0x4B400000;  // bit pattern of kRound
 // staged window (>= ceil(sqrt((TX-1)^2 + (TY-1)^2)) + 3 plus rounding margin:
 // the taps of every tile position lie in [ws, ws + span + 3)). MINB is the
 // launch-bounds occupancy target (registers 65536 / (256 MINB)).
-//
-// WALK shapes give each thread a column of VPT consecutive voxels along y
-// (lanes along x, XS = TX of them) instead of VPT voxels spaced along x.
-// Consecutive voxels of a column differ in detector coordinate by -sin(theta),
-// at most one bin, so walking them in increasing u the upper tap of one voxel
-// is mostly the lower tap of the next: the thread keeps its tap pair in
-// registers and loads a new tap only when floor(u) advances (on average
-// |sin theta| loads per voxel instead of two).
-template <int TX_, int TY_, int VPT_, int CA_, int WIN_, int MINB_, bool WALK_ = false>
+template <int TX_, int TY_, int VPT_, int CA_, int WIN_, int MINB_>
 struct Shape {
     static constexpr int TX = TX_, TY = TY_, VPT = VPT_, CA = CA_, WIN = WIN_, MINB = MINB_;
-    static constexpr bool WALK = WALK_;
-    static constexpr int XS = WALK ? TX : TX / VPT;  // lanes along x
-    static_assert(WALK ? TX * (TY / VPT) == THREADS : XS * TY == THREADS, "256 threads per CTA");
+    static constexpr int XS = TX / VPT;
+    static_assert(XS * TY == THREADS, "256 threads per CTA");
     static_assert(CA <= THREADS, "one thread per staged angle");
     static_assert(WIN <= kBpWindowMax, "window within the filtered-row guard");
 };
@@ -70,7 +61,6 @@ using V2 = Shape<32, 16, 2, 32, 40, 4>;  // half-height tiles: twice the CTAs
 using V3 = Shape<16, 16, 1, 32, 28, 4>;  // small tiles for small slices
 using V4 = Shape<32, 32, 4, 16, 52, 4>;  // the general shape with 16-angle chunks (half the staging buffer)
 using V5 = Shape<32, 32, 4, 64, 52, 2>;  // the general shape with 64-angle chunks (half the chunk barriers)
-using V6 = Shape<32, 32, 4, 32, 52, 4, true>;  // 32x32 tile, columns of 4 voxels walked along y
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -164,12 +154,8 @@ template <class C>
 __device__ __forceinline__ bool bp_tile(BpSmem<C>& S, const BpJob& J, int zg, int x0, int y0, unsigned& chunks,
                                         unsigned* err) {
     constexpr int TX = C::TX, TY = C::TY, VPT = C::VPT, XS = C::XS, CA = C::CA, WIN = C::WIN;
-    constexpr bool WALK = C::WALK;
     const int t = threadIdx.x;
     const int lx = t % XS, ly = t / XS;
-    // voxel k of this thread: (x0 + vox_dx(k), y0 + vox_dy(k))
-    auto vox_dx = [&](int k) { return WALK ? lx : lx + XS * k; };
-    auto vox_dy = [&](int k) { return WALK ? VPT * ly + k : ly; };
     const int n = J.n, nz = J.nz, na = J.na, sq = J.sq;
     const double ctr = J.ctr;  // voxel-grid centre (the mask radius too)
     const float radf = static_cast<float>(ctr);
@@ -193,9 +179,10 @@ __device__ __forceinline__ bool bp_tile(BpSmem<C>& S, const BpJob& J, int zg, in
         const double dx = fmax(0.0, fmax(x0 - ctr, ctr - xe));
         const double dy = fmax(0.0, fmax(y0 - ctr, ctr - ye));
         if (dx * dx + dy * dy > ctr * ctr) {
+            const int y = y0 + ly;
 #pragma unroll
             for (int k = 0; k < VPT; ++k) {
-                const int x = x0 + vox_dx(k), y = y0 + vox_dy(k);
+                const int x = x0 + lx + XS * k;
                 if (x >= n || y >= n) continue;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
@@ -246,16 +233,15 @@ __device__ __forceinline__ bool bp_tile(BpSmem<C>& S, const BpJob& J, int zg, in
     float4 acc[VPT];
 #pragma unroll
     for (int k = 0; k < VPT; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float fx = static_cast<float>(lx), fy = static_cast<float>(WALK ? VPT * ly : ly);
+    const float fx = static_cast<float>(lx), fy = static_cast<float>(ly);
     // positions inside the reconstruction circle (SerialBackend.cpp:220-224);
-    // the others are written as the offset only (their taps are never loaded,
-    // except as a walked column's intermediate taps)
+    // the others are written as the offset only, so their taps are never loaded
     unsigned inside_mask = 0;
     {
+        const float yy = static_cast<float>(y0 + ly) - radf;
 #pragma unroll
         for (int k = 0; k < VPT; ++k) {
-            const float xx = static_cast<float>(x0 + vox_dx(k)) - radf;
-            const float yy = static_cast<float>(y0 + vox_dy(k)) - radf;
+            const float xx = static_cast<float>(x0 + lx + XS * k) - radf;
             if (!(xx * xx + yy * yy > radf * radf)) inside_mask |= 1u << k;
         }
     }
@@ -276,67 +262,6 @@ __device__ __forceinline__ bool bp_tile(BpSmem<C>& S, const BpJob& J, int zg, in
             const float4* w = S.win[b][j];
             const float ub = fmaf(fx, r.c, fmaf(-fy, r.s, r.f0));
             const float c8 = static_cast<float>(XS) * r.c;
-            if constexpr (WALK) {
-                if (!r.edge) {
-                    // voxel k at u = ub - k s; walked in increasing u (k
-                    // descending when s >= 0: warp-uniform, one angle), so
-                    // floor(u) never decreases and rises by at most 1 per step
-                    // (2 only when rounding lands exactly on an integer)
-                    const bool desc = r.s >= 0.0f;
-                    const float ubh = ub - 0.5f;
-                    int ip = 0;
-                    float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
-#pragma unroll
-                    for (int st = 0; st < VPT; ++st) {
-                        const int k = desc ? VPT - 1 - st : st;
-                        const float uh = fmaf(static_cast<float>(k), -r.s, ubh);
-                        const float tr = uh + kRound;
-                        const int i = __float_as_int(tr) - kRoundBits;
-                        const float d = uh - (tr - kRound);  // frac(u) - 1/2
-                        const float w1 = d + 0.5f;
-                        const float w0 = 0.5f - d;
-                        if (st == 0) {
-                            lo = w[i];
-                            hi = w[i + 1];
-                        } else {
-                            const int dd = i - ip;
-                            if (dd == 1) lo = hi;
-                            if (dd > 1) lo = w[i];
-                            if (dd != 0) hi = w[i + 1];
-                        }
-                        ip = i;
-                        if (inside_mask & (1u << k)) {
-                            acc[k].x = fmaf(w1, hi.x, fmaf(w0, lo.x, acc[k].x));
-                            acc[k].y = fmaf(w1, hi.y, fmaf(w0, lo.y, acc[k].y));
-                            acc[k].z = fmaf(w1, hi.z, fmaf(w0, lo.z, acc[k].z));
-                            acc[k].w = fmaf(w1, hi.w, fmaf(w0, lo.w, acc[k].w));
-                        }
-                    }
-                } else {
-                    // detector edges: the reference's float u decides each
-                    // voxel's taps, as in the unwalked shapes
-#pragma unroll
-                    for (int k = 0; k < VPT; ++k) {
-                        if (!(inside_mask & (1u << k))) continue;
-                        const float u = fmaf(static_cast<float>(k), -r.s, ub);
-                        const float fl = floorf(u);
-                        const int i = static_cast<int>(fl);
-                        const float xs = static_cast<float>(x0 + vox_dx(k)) - radf;
-                        const float ys = static_cast<float>(y0 + vox_dy(k)) - radf;
-                        const float us = __fadd_rn(__fsub_rn(__fmul_rn(xs, r.cf), __fmul_rn(ys, r.sf)), dcf);
-                        const int is = static_cast<int>(floorf(us));
-                        const bool ok = (is >= 0) && (is + 1 < sq);
-                        const float w1 = ok ? u - fl : 0.0f;
-                        const float w0 = ok ? 1.0f - (u - fl) : 0.0f;
-                        const float4 lo = w[i], hi = w[i + 1];
-                        acc[k].x = fmaf(w1, hi.x, fmaf(w0, lo.x, acc[k].x));
-                        acc[k].y = fmaf(w1, hi.y, fmaf(w0, lo.y, acc[k].y));
-                        acc[k].z = fmaf(w1, hi.z, fmaf(w0, lo.z, acc[k].z));
-                        acc[k].w = fmaf(w1, hi.w, fmaf(w0, lo.w, acc[k].w));
-                    }
-                }
-                continue;
-            }
             if (!r.edge) {
                 // i = floor(u) by rounding u - 1/2 with the kRound addition (no
                 // conversion-unit instructions); at an exact tie u = i + 1 the taps
@@ -387,9 +312,10 @@ __device__ __forceinline__ bool bp_tile(BpSmem<C>& S, const BpJob& J, int zg, in
     }
     chunks += nch;
 
+    const int y = y0 + ly;
 #pragma unroll
     for (int k = 0; k < VPT; ++k) {
-        const int x = x0 + vox_dx(k), y = y0 + vox_dy(k);
+        const int x = x0 + lx + XS * k;
         if (x >= n || y >= n) continue;
         const bool inside = inside_mask & (1u << k);
         const float v[4] = {acc[k].x, acc[k].y, acc[k].z, acc[k].w};
@@ -509,7 +435,6 @@ BpShape bp_shape(int variant) {
     case 3: return shape_of<V3>();
     case 4: return shape_of<V4>();
     case 5: return shape_of<V5>();
-    case 6: return shape_of<V6>();
     default: return shape_of<V0>();
     }
 }
@@ -585,7 +510,6 @@ cudaError_t launch_backproject_batch(const BpBatch& b, int variant, unsigned* d_
     case 3: return launch_many<V3>(b, persistent, d_counter, d_err, st);
     case 4: return launch_many<V4>(b, persistent, d_counter, d_err, st);
     case 5: return launch_many<V5>(b, persistent, d_counter, d_err, st);
-    case 6: return launch_many<V6>(b, persistent, d_counter, d_err, st);
     default: return launch_many<V0>(b, persistent, d_counter, d_err, st);
     }
 }
@@ -604,7 +528,6 @@ cudaError_t launch_backproject(const float4* d_filt, int nz, int na, const FiltL
     case 3: return launch_one<V3>(b, d_err, st);
     case 4: return launch_one<V4>(b, d_err, st);
     case 5: return launch_one<V5>(b, d_err, st);
-    case 6: return launch_one<V6>(b, d_err, st);
     default: return launch_one<V0>(b, d_err, st);
     }
 }

@@ -52,7 +52,7 @@ FiltLayout filt_layout(int sq, int n_out);
 
 // Backprojection tile shapes ("variants"): tx x ty voxels, vpt voxels per
 // thread, ca angles per staged chunk, win bins per staged window.
-constexpr int kBpVariants = 7;
+constexpr int kBpVariants = 6;
 struct BpShape {
     int tx, ty, vpt, ca, win;
 };
