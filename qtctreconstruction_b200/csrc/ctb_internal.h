@@ -136,20 +136,19 @@ cudaError_t launch_filter(const float* d_sino, int nz, int na, const PadGeom& g,
                           cudaStream_t st);
 
 // ------------------------------------------------ tensor-core filter option
-// Toeplitz filter matrix T[i][j] = h(i - pad - j) split into two BF16 terms
-// (rows padded to ntiles * bn, columns to kpad), with the TMA tensor maps of
-// both halves (opaque CUtensorMap bytes).
+// Toeplitz filter matrix T[i][j] = h(i - pad - j) split into three BF16 terms
+// (rows padded to ntiles * bn, columns to kpad), with the TMA tensor map of
+// each term (opaque CUtensorMap bytes).
 struct GemmTable {
     DevBuf T;
     int bn = 0, ntiles = 0, nrows = 0, kpad = 0;
-    alignas(64) unsigned char map_hi[128];
-    alignas(64) unsigned char map_lo[128];
+    alignas(64) unsigned char map[3][128];
 };
 cudaError_t make_gemm_table(const PadGeom& g, int type, bool keep_nyquist, GemmTable* out);
 int gemm_kpad(int bins);
-// Device bytes of the BF16 row split the tensor-core filter needs.
+// Device bytes of the three-term BF16 row split the tensor-core filter needs.
 size_t filter_gemm_split_bytes(int nz, int na, int bins);
-// Operand split (two BF16 terms of every row) and the zero guard bins; then
+// Operand split (three BF16 terms of every row) and the zero guard bins; then
 // the tensor-core product itself.
 cudaError_t launch_filter_gemm_prep(const float* d_sino, int nz, int na, const PadGeom& g, const FiltLayout& fl,
                                     const GemmTable& tab, float4* d_filt, void* d_split, cudaStream_t st);

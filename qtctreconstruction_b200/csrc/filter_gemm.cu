@@ -6,15 +6,18 @@
 // Filtered bin i of a sinogram row x is y[i] = sum_j h(i - pad - j) x[j] with
 // the lag-domain kernel h of conv_kernel (the same linear operator the FFT
 // path applies). Over all rows this is Y[rows x sq] = X[rows x nd] T^T with the
-// Toeplitz matrix T[i][j] = h(i - pad - j). Both factors are split into two
-// BF16 terms, X = Xh + Xl and T = Th + Tl, and the product is accumulated in
-// FP32 in tensor memory as Xh Th + Xh Tl + Xl Th (the Xl Tl term, about 2^-16
-// relative, is dropped).
+// Toeplitz matrix T[i][j] = h(i - pad - j). Both factors are split into three
+// BF16 terms, X = X0 + X1 + X2 and T = T0 + T1 + T2 (each term the BF16
+// rounding of what the previous ones leave, about 24 significant bits in
+// all), and the six products Xa Tb with a + b <= 2 are accumulated in FP32 in
+// tensor memory, smallest first (the dropped terms are about 2^-24 relative).
+// Two-term splitting, 16 bits, is not enough: the ramp filter's cancellation
+// amplifies its error to ~1e-4 rel-L2 of the reconstruction.
 //
-// Kernel shape: one CTA per 128-row x BN-bin output tile (BN <= 256, a multiple
-// of 16 chosen so that ceil(sq / 256) tiles cover sq with the least waste),
-// 128 threads. Thread 0 stages 64-wide K slices of Xh, Xl, Th, Tl with TMA
-// (cp.async.bulk.tensor, 128-byte swizzle, no multicast) into a two-stage ring;
+// Kernel shape: one CTA per 128-row x BN-bin output tile (BN <= 160, a multiple
+// of 16 chosen so that ceil(sq / 160) tiles cover sq with the least waste),
+// 128 threads. Thread 0 stages 64-wide K slices of the six operand terms with
+// TMA (cp.async.bulk.tensor, 128-byte swizzle, no multicast) into a two-stage ring;
 // thread 32 issues tcgen05.mma (kind::f16, BF16 in, FP32 accumulate, M = 128,
 // N = BN, K = 16) from shared-memory descriptors and releases each stage with
 // tcgen05.commit; after the last slice all four warps read the accumulator
@@ -39,11 +42,13 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BK = 64;          // bf16 per 128-byte swizzle row
-constexpr int BNMAX = 256;
+constexpr int BNMAX = 160;
 constexpr int STAGES = 2;
+constexpr int NTERMS = 3;                // BF16 terms per factor
 constexpr int A_BYTES = BM * BK * 2;     // 16 KB
-constexpr int B_BYTES = BNMAX * BK * 2;  // 32 KB
-constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+constexpr int B_BYTES = BNMAX * BK * 2;  // 20 KB
+constexpr int STAGE_BYTES = NTERMS * A_BYTES + NTERMS * B_BYTES;  // 108 KB: two stages fit
+static_assert(A_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "operand tiles on the 1024-byte swizzle atom");
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + 1024-byte alignment slack
 constexpr int TMEM_COLS = 256;
 constexpr unsigned kWaitLimit = 1u << 22;
@@ -149,10 +154,12 @@ __device__ __forceinline__ float row_scale(const float4* stats, int z, int nz, i
     return span > 0.0f ? scale * span : 0.0f;
 }
 
-__global__ void __launch_bounds__(128, 1) k_filter_gemm(const __grid_constant__ CUtensorMap mapXh,
-                                                        const __grid_constant__ CUtensorMap mapXl,
-                                                        const __grid_constant__ CUtensorMap mapTh,
-                                                        const __grid_constant__ CUtensorMap mapTl,
+// The tensor maps of the six operand terms (X0, X1, X2, T0, T1, T2).
+struct GemmMaps {
+    CUtensorMap x[NTERMS], t[NTERMS];
+};
+
+__global__ void __launch_bounds__(128, 1) k_filter_gemm(const __grid_constant__ GemmMaps maps,
                                                         const GemmParams P, unsigned* __restrict__ err) {
     extern __shared__ unsigned char smem_raw[];
     // 1024-byte alignment of the shared-window offset (the swizzle atom)
@@ -182,7 +189,7 @@ __global__ void __launch_bounds__(128, 1) k_filter_gemm(const __grid_constant__ 
     __syncthreads();
     tc_fence_after();
     const unsigned tmem = tmem_slot;
-    const unsigned tx_bytes = 2u * A_BYTES + 2u * static_cast<unsigned>(P.bn) * BK * 2u;
+    const unsigned tx_bytes = NTERMS * A_BYTES + NTERMS * static_cast<unsigned>(P.bn) * BK * 2u;
 
     if (threadIdx.x == 0) {
         // producer: K slice kt into stage kt % STAGES once the MMAs of slice
@@ -196,10 +203,11 @@ __global__ void __launch_bounds__(128, 1) k_filter_gemm(const __grid_constant__ 
             }
             unsigned char* st = smem + s * STAGE_BYTES;
             mbar_expect_tx(&full[s], tx_bytes);
-            tma_load_2d(st, &mapXh, kt * BK, m0, &full[s]);
-            tma_load_2d(st + A_BYTES, &mapXl, kt * BK, m0, &full[s]);
-            tma_load_2d(st + 2 * A_BYTES, &mapTh, kt * BK, n0, &full[s]);
-            tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mapTl, kt * BK, n0, &full[s]);
+#pragma unroll
+            for (int a = 0; a < NTERMS; ++a) tma_load_2d(st + a * A_BYTES, &maps.x[a], kt * BK, m0, &full[s]);
+#pragma unroll
+            for (int b = 0; b < NTERMS; ++b)
+                tma_load_2d(st + NTERMS * A_BYTES + b * B_BYTES, &maps.t[b], kt * BK, n0, &full[s]);
             issued = kt + 1;
         }
         if (issued < P.nk) {
@@ -208,7 +216,8 @@ __global__ void __launch_bounds__(128, 1) k_filter_gemm(const __grid_constant__ 
                 mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1);
         }
     } else if (threadIdx.x == 32) {
-        // MMA issuer: 3 products x 4 K steps of 16 per slice
+        // MMA issuer: 6 products x 4 K steps of 16 per slice, the products of
+        // the smaller terms first (a + b = 2, then 1, then 0)
         const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<unsigned>(P.bn >> 3) << 17) |
                                (static_cast<unsigned>(BM >> 4) << 24);
         for (int kt = 0; kt < P.nk; ++kt) {
@@ -219,14 +228,11 @@ __global__ void __launch_bounds__(128, 1) k_filter_gemm(const __grid_constant__ 
             }
             tc_fence_after();
             const unsigned char* st = smem + s * STAGE_BYTES;
-            const unsigned char* xh = st;
-            const unsigned char* xl = st + A_BYTES;
-            const unsigned char* th = st + 2 * A_BYTES;
-            const unsigned char* tl = th + B_BYTES;
+            constexpr int PA[6] = {2, 1, 0, 1, 0, 0}, PB[6] = {0, 1, 2, 0, 1, 0};
 #pragma unroll
-            for (int p = 0; p < 3; ++p) {
-                const unsigned char* a = p == 2 ? xl : xh;
-                const unsigned char* b = p == 1 ? tl : th;
+            for (int p = 0; p < 6; ++p) {
+                const unsigned char* a = st + PA[p] * A_BYTES;
+                const unsigned char* b = st + NTERMS * A_BYTES + PB[p] * B_BYTES;
 #pragma unroll
                 for (int ks = 0; ks < BK / 16; ++ks)
                     mma_bf16(tmem, smem_desc(a + ks * 32), smem_desc(b + ks * 32), idesc,
@@ -280,11 +286,12 @@ __global__ void __launch_bounds__(128, 1) k_filter_gemm(const __grid_constant__ 
                      : "memory");
 }
 
-// X rows in (slice group, angle, slice % 4) order, split into two BF16 terms;
-// K padded with zeros to kpad, rows past the last slice zero.
+// X rows in (slice group, angle, slice % 4) order, split into three BF16
+// terms (x0 = bf16(x), x1 = bf16(x - x0), x2 = bf16(x - x0 - x1); the
+// differences are exact in float); K padded with zeros to kpad, rows past the
+// last slice zero. The terms are stored one after the other, rows x kpad each.
 __global__ void __launch_bounds__(256) k_split_rows(const float* __restrict__ sino, int nz, int na, int nd,
-                                                    int kpad, long long rows, __nv_bfloat16* __restrict__ xh,
-                                                    __nv_bfloat16* __restrict__ xl) {
+                                                    int kpad, long long rows, __nv_bfloat16* __restrict__ x0) {
     const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     const long long per_row = kpad / 8;
     if (i >= rows * per_row) return;
@@ -293,16 +300,21 @@ __global__ void __launch_bounds__(256) k_split_rows(const float* __restrict__ si
     const int pair = static_cast<int>(r >> 2), q = static_cast<int>(r & 3);
     const int z = 4 * (pair / na) + q, a = pair % na;
     const float* src = sino + (static_cast<long long>(z) * na + a) * nd;
-    __align__(16) __nv_bfloat16 h[8], l[8];
+    __align__(16) __nv_bfloat16 term[NTERMS][8];
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
         const int k = k0 + t;
-        const float x = (z < nz && k < nd) ? src[k] : 0.0f;
-        h[t] = __float2bfloat16_rn(x);
-        l[t] = __float2bfloat16_rn(x - __bfloat162float(h[t]));
+        float x = (z < nz && k < nd) ? src[k] : 0.0f;
+#pragma unroll
+        for (int a = 0; a < NTERMS; ++a) {
+            term[a][t] = __float2bfloat16_rn(x);
+            x -= __bfloat162float(term[a][t]);
+        }
     }
-    *reinterpret_cast<uint4*>(xh + r * kpad + k0) = *reinterpret_cast<const uint4*>(h);
-    *reinterpret_cast<uint4*>(xl + r * kpad + k0) = *reinterpret_cast<const uint4*>(l);
+    const long long plane = rows * kpad;
+#pragma unroll
+    for (int a = 0; a < NTERMS; ++a)
+        *reinterpret_cast<uint4*>(x0 + a * plane + r * kpad + k0) = *reinterpret_cast<const uint4*>(term[a]);
 }
 
 // Round-to-nearest-even float -> bf16 bits (finite inputs).
@@ -355,40 +367,44 @@ int gemm_kpad(int bins) { return (bins + BK - 1) / BK * BK; }
 
 size_t filter_gemm_split_bytes(int nz, int na, int bins) {
     const long long rows = (static_cast<long long>((nz + 3) / 4) * na * 4 + BM - 1) / BM * BM;
-    return static_cast<size_t>(rows) * gemm_kpad(bins) * 2 * sizeof(__nv_bfloat16);
+    return static_cast<size_t>(rows) * gemm_kpad(bins) * NTERMS * sizeof(__nv_bfloat16);
 }
 
 cudaError_t make_gemm_table(const PadGeom& g, int type, bool keep_nyquist, GemmTable* out) {
-    static_assert(sizeof(CUtensorMap) == sizeof(out->map_hi), "tensor map size");
+    static_assert(sizeof(CUtensorMap) == sizeof(out->map[0]), "tensor map size");
+    static_assert(sizeof(out->map) / sizeof(out->map[0]) == NTERMS, "one map per term");
     const int ntiles = (g.sq + BNMAX - 1) / BNMAX;
     const int bn = 16 * ((g.sq + 16 * ntiles - 1) / (16 * ntiles));
     const int nrows = ntiles * bn;
     const int kpad = gemm_kpad(g.bins);
     const std::vector<double> h = conv_kernel(g, type, keep_nyquist);
     const int dmin = -(g.pad + g.bins - 1);
-    std::vector<unsigned short> th(static_cast<size_t>(nrows) * kpad, 0), tl(th.size(), 0);
+    // T's three BF16 terms, each the rounding of what the previous ones leave
+    // (in double), stored one after the other
+    const size_t plane = static_cast<size_t>(nrows) * kpad;
+    std::vector<unsigned short> tt(NTERMS * plane, 0);
     for (int i = 0; i < g.sq; ++i)
         for (int j = 0; j < g.bins; ++j) {
-            const double t = h[i - g.pad - j - dmin];
-            const unsigned short hb = bf16_bits(static_cast<float>(t));
-            th[static_cast<size_t>(i) * kpad + j] = hb;
-            tl[static_cast<size_t>(i) * kpad + j] = bf16_bits(static_cast<float>(t - bf16_value(hb)));
+            double t = h[i - g.pad - j - dmin];
+            for (int a = 0; a < NTERMS; ++a) {
+                const unsigned short b = bf16_bits(static_cast<float>(t));
+                tt[a * plane + static_cast<size_t>(i) * kpad + j] = b;
+                t -= bf16_value(b);
+            }
         }
-    const size_t bytes = th.size() * 2;
+    const size_t bytes = plane * 2;
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, 2 * bytes);
+    cudaError_t e = cudaMalloc(&p, NTERMS * bytes);
     if (e != cudaSuccess) return e;
-    e = cudaMemcpy(p, th.data(), bytes, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(static_cast<char*>(p) + bytes, tl.data(), bytes, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && (!encode_map(out->map_hi, p, nrows, kpad, bn) ||
-                             !encode_map(out->map_lo, static_cast<char*>(p) + bytes, nrows, kpad, bn)))
-        e = cudaErrorNotSupported;
+    e = cudaMemcpy(p, tt.data(), NTERMS * bytes, cudaMemcpyHostToDevice);
+    for (int a = 0; a < NTERMS && e == cudaSuccess; ++a)
+        if (!encode_map(out->map[a], static_cast<char*>(p) + a * bytes, nrows, kpad, bn)) e = cudaErrorNotSupported;
     if (e != cudaSuccess) {
         cudaFree(p);
         return e;
     }
     out->T.ptr = p;
-    out->T.bytes = 2 * bytes;
+    out->T.bytes = NTERMS * bytes;
     out->bn = bn;
     out->ntiles = ntiles;
     out->nrows = nrows;
@@ -402,11 +418,10 @@ cudaError_t launch_filter_gemm_prep(const float* d_sino, int nz, int na, const P
     const long long pairs = static_cast<long long>(nzg) * na;
     const long long rows = (pairs * 4 + BM - 1) / BM * BM;
     if (rows / BM > 65535) return cudaErrorInvalidValue;
-    __nv_bfloat16* xh = static_cast<__nv_bfloat16*>(d_split);
-    __nv_bfloat16* xl = xh + rows * tab.kpad;
+    __nv_bfloat16* x0 = static_cast<__nv_bfloat16*>(d_split);
     const long long items = rows * (tab.kpad / 8);
     k_split_rows<<<static_cast<unsigned>((items + 255) / 256), 256, 0, st>>>(d_sino, nz, na, g.bins, tab.kpad,
-                                                                              rows, xh, xl);
+                                                                              rows, x0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // zero guard bins on both sides of every filtered row
@@ -428,14 +443,13 @@ cudaError_t launch_filter_gemm(const float* d_sino, int nz, int na, const PadGeo
     const long long rows = (pairs * 4 + BM - 1) / BM * BM;
     if (rows / BM > 65535 || pairs > 0x7fffffffLL) return cudaErrorInvalidValue;
     (void)d_sino;
-    const __nv_bfloat16* xh = static_cast<const __nv_bfloat16*>(d_split);
-    const __nv_bfloat16* xl = xh + rows * tab.kpad;
+    const __nv_bfloat16* x0 = static_cast<const __nv_bfloat16*>(d_split);
     cudaError_t e;
-    CUtensorMap mxh, mxl, mth, mtl;
-    if (!encode_map(&mxh, xh, rows, tab.kpad, BM) || !encode_map(&mxl, xl, rows, tab.kpad, BM))
-        return cudaErrorNotSupported;
-    std::memcpy(&mth, tab.map_hi, sizeof mth);
-    std::memcpy(&mtl, tab.map_lo, sizeof mtl);
+    GemmMaps maps;
+    for (int a = 0; a < NTERMS; ++a) {
+        if (!encode_map(&maps.x[a], x0 + a * rows * tab.kpad, rows, tab.kpad, BM)) return cudaErrorNotSupported;
+        std::memcpy(&maps.t[a], tab.map[a], sizeof maps.t[a]);
+    }
     GemmParams P;
     P.filt = d_filt;
     P.stats = d_stats;
@@ -452,7 +466,7 @@ cudaError_t launch_filter_gemm(const float* d_sino, int nz, int na, const PadGeo
     e = cudaFuncSetAttribute(k_filter_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     if (e != cudaSuccess) return e;
     const dim3 grid(tab.ntiles, static_cast<unsigned>(rows / BM));
-    k_filter_gemm<<<grid, 128, SMEM_BYTES, st>>>(mxh, mxl, mth, mtl, P, d_err);
+    k_filter_gemm<<<grid, 128, SMEM_BYTES, st>>>(maps, P, d_err);
     return cudaGetLastError();
 }
 
