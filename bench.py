@@ -786,6 +786,25 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
         ms_t = e0.elapsed_time(e1) / args.steps
     be.set_autotune(False)
     results["graph_autotuned"] = dict(ms_per_step=ms_t, value=updates / (ms_t * 1e-3))
+    # accuracy of the batch's outputs at the mix's sizes: the first slice of the
+    # largest and of the middle job against the FP64 rerun (sinograms from the
+    # device, oracle in threads)
+    import concurrent.futures as cf
+
+    import oracle as O
+    with be.batch(jobs, ctb.BATCH_GRAPH) as b:
+        b.run()
+        torch.cuda.synchronize()
+
+    def check(k):
+        s = shapes[k]
+        sino, out = keep[k]
+        ang = O.uniform_angles_deg(s["na"])
+        f64 = O.reconstruct_slice_f64(sino[0].double().cpu().numpy(), ang, s["n"], s["filter"])
+        got = out[0].cpu().numpy()
+        return {"job": s, "rel_l2_vs_fp64": O.rel_l2(got, f64), "max_abs_vs_fp64": O.max_abs_rel(got, f64)}
+    with cf.ThreadPoolExecutor(max_workers=2) as ex:
+        accuracy = list(ex.map(check, (order[-1], order[len(order) // 2])))
     g = results["graph"]
     line = {
         "metric": METRIC, "value": g["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
@@ -799,6 +818,7 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
         "modes": results,
         "batched_vs_per_job": results["per_job"]["ms_per_step"] / g["ms_per_step"],
         "outputs_identical_across_modes": same,
+        "accuracy": accuracy,
         "autotune_table": [dict(zip(("n_bucket", "angle_bucket", "depth_bucket", "shape"), e)) for e in table],
         "shape_times": shape_times,
         "clocks": g.get("clocks"),

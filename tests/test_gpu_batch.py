@@ -128,3 +128,51 @@ def test_batch_rejects_bad_jobs(backend):
     with pytest.raises(ctb.CtbError) as e:
         backend.fbp_batch_d([big])
     assert e.value.status == 4
+
+
+def test_batch_at_the_mix_largest_sizes_against_fp64(backend):
+    """The largest job sizes of the batch mix (n = 768, 1206 angles, 1087
+    bins, Hann; n = 736, 1156 angles, Shepp-Logan) batched with small jobs,
+    held to the FP64 rerun of SerialBackend's reconstructSlice at rel-L2 <=
+    1e-5 and max-abs <= 1e-4 * max|f| (at these sizes SerialBackend's own float
+    rounding is near 1e-5, so it is reported against, not gated)."""
+    import concurrent.futures as cf
+    import torch
+    rng = np.random.default_rng(16)
+    big = [(768, 2, 1206, FilterType.Hann), (736, 2, 1156, FilterType.SheppLogan)]
+    jobs, host = [], []
+    for n, depth, na, kind in big:
+        nd = ctb.odd_detector_count(n)
+        yy, xx = np.mgrid[0:n, 0:n].astype(np.float64)
+        sl = []
+        for _ in range(depth):
+            s = np.zeros((n, n), np.float32)
+            for _ in range(5):
+                cx, cy = rng.uniform(0.3 * n, 0.7 * n, 2)
+                a, b = rng.uniform(0.05 * n, 0.2 * n, 2)
+                s[((xx - cx) / a) ** 2 + ((yy - cy) / b) ** 2 <= 1.0] += np.float32(rng.uniform(-0.3, 1.0))
+            sl.append(s)
+        sino = np.stack([O.sinogram_f32(s, na, nd)[0] for s in sl])
+        d_sino = torch.from_numpy(sino).cuda()
+        d_out = torch.full((depth, n, n), float("nan"), dtype=torch.float32, device="cuda")
+        host.append(dict(sino=sino, n=n, kind=kind, d_out=d_out, d_sino=d_sino))
+        jobs.append(dict(sino=d_sino.data_ptr(), depth=depth, num_angles=na, bins=nd, output_size=n,
+                         filter=int(kind), out=d_out.data_ptr()))
+    small_jobs, small_host = _make_jobs(torch, SHAPES[:3], 17)
+    backend.fbp_batch_d(jobs + small_jobs)
+    work = [(h, z) for h in host for z in range(h["sino"].shape[0])]
+
+    def oracle(hz):
+        h, z = hz
+        ang = O.uniform_angles_deg(h["sino"].shape[1])
+        return (O.reconstruct_slice_f64(h["sino"][z].astype(np.float64), ang, h["n"], int(h["kind"])),
+                O.reconstruct_slice_f32(h["sino"][z], ang, h["n"], int(h["kind"])))
+    with cf.ThreadPoolExecutor(max_workers=4) as ex:
+        refs = list(ex.map(oracle, work))
+    for (h, z), (f64, f32) in zip(work, refs):
+        got = h["d_out"].cpu().numpy()[z]
+        assert np.all(np.isfinite(got))
+        assert O.rel_l2(got, f64) <= REL_L2, (h["n"], z, O.rel_l2(got, f64), O.rel_l2(f32, f64))
+        assert O.max_abs_rel(got, f64) <= MAX_ABS
+    for h in small_host:
+        np.testing.assert_array_equal(h["d_out"].cpu().numpy(), _alone(backend, torch, h))
