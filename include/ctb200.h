@@ -110,9 +110,10 @@ ctb_status ctb_filter_kernel_ms(ctb_ctx* ctx, int back, double* ms);
  * ctb_fbp*, the _d variants; batches and the serving loop always use the FFT):
  *   FFT         the radix-16 shared-memory FFT convolution in FP32 (default);
  *   TC_BF16X3   the same linear operator as a dense Toeplitz-matrix product on
- *               the tcgen05 tensor cores, both factors split into two BF16
- *               terms, three products accumulated in FP32 (the precision
- *               option; the dropped low x low term is about 2^-16 relative).
+ *               the tcgen05 tensor cores, both factors split into three BF16
+ *               terms (about 24 significant bits), the six products whose
+ *               terms' orders add up to at most 2 accumulated in FP32 (the
+ *               dropped ones are about 2^-24 relative).
  * The reference filters with its own radix-2 FFT (FFT.cpp:9-158). */
 enum { CTB_FILTER_MODE_FFT = 0, CTB_FILTER_MODE_TC_BF16X3 = 1 };
 ctb_status ctb_set_filter_mode(ctb_ctx* ctx, int mode);
