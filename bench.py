@@ -632,13 +632,13 @@ def filter_mode_report(args, cfg, be, stream, vol, out, params, peaks):
         km = float(np.mean([be.filter_kernel_ms(b) for b in range(steps)]))
         rep[name] = {"filter_stage_ms": float(st[2]), "main_kernel_ms": km}
     be.set_filter_mode(ctb.FILTER_MODE_FFT)
-    flops = 3 * 2.0 * nz * na * nd * sq
+    flops = 6 * 2.0 * nz * na * nd * sq
     tc_ms = rep["tc_bf16x3"]["main_kernel_ms"]
     peak = peaks.get("bf16_tflops_sustained")
     rep["tc_bf16x3"]["roofline"] = {
         "kernel": "k_filter_gemm", "bound": "tensor", "achieved": flops / (tc_ms * 1e-3) / 1e12, "peak": peak,
         "unit": "TFLOP/s", "frac": (flops / (tc_ms * 1e-3) / 1e12 / peak) if peak else None,
-        "algorithmic": "3 x 2 x rows x nd x sq FLOP (three BF16 products of the Toeplitz filter)",
+        "algorithmic": "6 x 2 x rows x nd x sq FLOP (six BF16 products of the three-term Toeplitz filter)",
         "peak_source": "bf16_tflops_sustained (the kernel runs inside a long step), " + peaks["_label"]}
     # accuracy on two slices against the FP64 rerun
     z0 = nz // 2
