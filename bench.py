@@ -630,16 +630,21 @@ def filter_mode_report(args, cfg, be, stream, vol, out, params, peaks):
         torch.cuda.synchronize()
         st = np.mean([be.stage_times(b) for b in range(steps)], axis=0)
         km = float(np.mean([be.filter_kernel_ms(b) for b in range(steps)]))
-        rep[name] = {"filter_stage_ms": float(st[2]), "main_kernel_ms": km}
+        rep[name] = {"filter_stage_ms": float(st[2]), "main_kernel_ms": km, "step_ms": float(np.sum(st))}
     be.set_filter_mode(ctb.FILTER_MODE_FFT)
     flops = 6 * 2.0 * nz * na * nd * sq
     tc_ms = rep["tc_bf16x3"]["main_kernel_ms"]
-    peak = peaks.get("bf16_tflops_sustained")
+    # the sustained GEMM figure for a kernel inside a step of 100 ms or more
+    # (the GPU settles under its power cap), the burst figure for a short one
+    long_step = rep["tc_bf16x3"]["step_ms"] >= 100.0
+    peak_key = "bf16_tflops_sustained" if long_step else "bf16_tflops"
+    peak = peaks.get(peak_key)
     rep["tc_bf16x3"]["roofline"] = {
         "kernel": "k_filter_gemm", "bound": "tensor", "achieved": flops / (tc_ms * 1e-3) / 1e12, "peak": peak,
         "unit": "TFLOP/s", "frac": (flops / (tc_ms * 1e-3) / 1e12 / peak) if peak else None,
         "algorithmic": "6 x 2 x rows x nd x sq FLOP (six BF16 products of the three-term Toeplitz filter)",
-        "peak_source": "bf16_tflops_sustained (the kernel runs inside a long step), " + peaks["_label"]}
+        "peak_source": (f"{peak_key} (the kernel runs inside a {rep['tc_bf16x3']['step_ms']:.1f} ms step), "
+                        + peaks["_label"])}
     # accuracy on two slices against the FP64 rerun
     z0 = nz // 2
     slab = torch.from_numpy(O.phantom_sum_slab(params, n, n, nz, z0, 2)).cuda()
@@ -786,9 +791,9 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
         ms_t = e0.elapsed_time(e1) / args.steps
     be.set_autotune(False)
     results["graph_autotuned"] = dict(ms_per_step=ms_t, value=updates / (ms_t * 1e-3))
-    # accuracy of the batch's outputs at the mix's sizes: the first slice of the
-    # largest and of the middle job against the FP64 rerun (sinograms from the
-    # device, oracle in threads)
+    # accuracy of the batch's outputs at the mix's sizes: the central slice of
+    # the largest and of the middle job against the FP64 rerun (sinograms from
+    # the device, oracle in threads; the phantoms' end slices can be empty)
     import concurrent.futures as cf
 
     import oracle as O
@@ -799,10 +804,12 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
     def check(k):
         s = shapes[k]
         sino, out = keep[k]
+        z = s["nz"] // 2
         ang = O.uniform_angles_deg(s["na"])
-        f64 = O.reconstruct_slice_f64(sino[0].double().cpu().numpy(), ang, s["n"], s["filter"])
-        got = out[0].cpu().numpy()
-        return {"job": s, "rel_l2_vs_fp64": O.rel_l2(got, f64), "max_abs_vs_fp64": O.max_abs_rel(got, f64)}
+        f64 = O.reconstruct_slice_f64(sino[z].double().cpu().numpy(), ang, s["n"], s["filter"])
+        got = out[z].cpu().numpy()
+        return {"job": s, "slice": z, "max_abs_fp64": float(abs(f64).max()),
+                "rel_l2_vs_fp64": O.rel_l2(got, f64), "max_abs_vs_fp64": O.max_abs_rel(got, f64)}
     with cf.ThreadPoolExecutor(max_workers=2) as ex:
         accuracy = list(ex.map(check, (order[-1], order[len(order) // 2])))
     g = results["graph"]
