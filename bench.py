@@ -791,9 +791,10 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
         ms_t = e0.elapsed_time(e1) / args.steps
     be.set_autotune(False)
     results["graph_autotuned"] = dict(ms_per_step=ms_t, value=updates / (ms_t * 1e-3))
-    # accuracy of the batch's outputs at the mix's sizes: the central slice of
-    # the largest and of the middle job against the FP64 rerun (sinograms from
-    # the device, oracle in threads; the phantoms' end slices can be empty)
+    # accuracy of the batch's outputs at the mix's sizes: the slice with the
+    # largest sinogram of the largest and of the middle job against the FP64
+    # rerun (sinograms from the device, oracle in threads; a phantom of 10
+    # ellipsoids leaves many slices empty)
     import concurrent.futures as cf
 
     import oracle as O
@@ -804,7 +805,7 @@ def run_batch(args, cfg, rank: int, world: int, local: int):
     def check(k):
         s = shapes[k]
         sino, out = keep[k]
-        z = s["nz"] // 2
+        z = int(torch.argmax(sino.abs().sum(dim=(1, 2))))  # the slice with the most signal
         ang = O.uniform_angles_deg(s["na"])
         f64 = O.reconstruct_slice_f64(sino[z].double().cpu().numpy(), ang, s["n"], s["filter"])
         got = out[z].cpu().numpy()

@@ -180,6 +180,7 @@ ctb_status forward_plan_dev(ctb_ctx* ctx, const float* angles_deg, int na, int w
         const FwdPlan plan = forward_plan(angles_deg, na, w, h, nd);
         ctb_ctx::FwdPlanDev d;
         d.ngroups = static_cast<int>(plan.groups.size() / 4);
+        d.max_strips = plan.max_strips;
         CTB_CUDA(ctx, cudaMalloc(&d.groups.ptr, sizeof(int) * plan.groups.size()));
         CTB_CUDA(ctx, cudaMalloc(&d.order.ptr, sizeof(int) * plan.order.size()));
         CTB_CUDA(ctx, cudaMemcpy(d.groups.ptr, plan.groups.data(), sizeof(int) * plan.groups.size(),
@@ -199,7 +200,7 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
                          const float* angles_deg, float* d_sino, float4* d_stats,
                          cudaEvent_t* ev = nullptr, bool volume_path = false) {
     const int nzg = (nz + 3) / 4;
-    const size_t elems = static_cast<size_t>(nzg) * std::max(fwd_plane_elems(h, w), fwd_plane_elems(w, h));
+    const size_t elems = fwd_plane_count(nz) * std::max(fwd_plane_elems(h, w), fwd_plane_elems(w, h));
     CTB_WS(ctx, d_img, float4, "img", elems);
     CTB_WS(ctx, d_imgT, float4, "imgT", elems);
     CTB_WS(ctx, d_box, int4, "fbox", 2 * nzg);  // per group: box, then disc
@@ -237,7 +238,7 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     const ctb_ctx::FwdPlanDev* plan = nullptr;
     CTB_TRY(forward_plan_dev(ctx, angles_deg, na, w, h, nd, &plan));
     CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd, trig,
-                                   static_cast<const int4*>(plan->groups.ptr), plan->ngroups,
+                                   static_cast<const int4*>(plan->groups.ptr), plan->ngroups, plan->max_strips,
                                    static_cast<const int*>(plan->order.ptr), box, band, d_sino,
                                    ctx->stream));
     return CTB_OK;
@@ -249,7 +250,7 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
 // device) between its launches.
 ctb_status reserve_volume_workspaces(ctb_ctx* ctx, int n, int nz_max, int na, int nd) {
     const int nzg = (nz_max + 3) / 4;
-    const size_t elems = static_cast<size_t>(nzg) * fwd_plane_elems(n, n);
+    const size_t elems = fwd_plane_count(nz_max) * fwd_plane_elems(n, n);
     const int nband = 2 * ((n + 7) / 8);
     CTB_WS(ctx, d_img, float4, "img", elems);
     CTB_WS(ctx, d_imgT, float4, "imgT", elems);

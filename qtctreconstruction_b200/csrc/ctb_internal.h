@@ -96,25 +96,38 @@ cudaError_t launch_raymarch(const float4* d_img, int w, int h, int nz, int na, i
 // Forward projector work plan: angles grouped (up to kFwdGroup per CTA, in
 // their given order) by walked axis, so that the angles of a CTA read the
 // same image rows at the same time. groups: {first index into order, count,
-// axis (0 rows, 1 columns), 0}.
-constexpr int kFwdRays = 32;   // detector intervals per CTA (kFwdRays - 1 output bins)
-constexpr int kFwdRows = 16;   // walked rows per chunk (boundaries in double once per chunk)
+// axis (0 rows, 1 columns), K}, K the output bins per strip of the group
+// (fwd_strip_bins of its smallest |kq|); max_strips = ceil(nd / smallest K).
+constexpr int kFwdRows = 16;   // walked rows per chunk (crossing in double once per chunk)
 constexpr int kFwdGroup = 4;   // angles per CTA
 constexpr int kFwdPlanes = 2;  // float4 image planes (4 slices each) per thread
 // Zero border of the normalised image planes: kFwdGuard pixels on both sides
-// of every row and kFwdRows rows after the last, so that every chunk the
+// of every row (a warp's 32 columns, clamped into it where the strip leaves
+// the image) and kFwdRows rows after the last, so that every chunk the
 // projector walks reads inside the plane.
-constexpr int kFwdGuard = kFwdRows + 8;
+constexpr int kFwdGuard = 32;
 inline size_t fwd_plane_elems(int np, int nq) {
     return static_cast<size_t>(np + kFwdRows) * static_cast<size_t>(nq + 2 * kFwdGuard);
 }
+// Float4 planes allocated for nz slices: whole groups of kFwdPlanes, since a
+// projector CTA reads all planes of its group.
+inline size_t fwd_plane_count(int nz) {
+    const int ng4 = (nz + 3) / 4;
+    return static_cast<size_t>((ng4 + kFwdPlanes - 1) / kFwdPlanes * kFwdPlanes);
+}
+// Output bins per strip for a walked-axis coefficient |kq| (>= 1/sqrt 2): the
+// 32 lanes of a warp cover bins -1/2 |kq| .. 31.5 |kq| above the strip's lower
+// edge, which must hold the strip's K bins and one bin on each side with a
+// bin to spare: K = floor(31.5 |kq|) - 2.
+inline int fwd_strip_bins(double akq) { return static_cast<int>(std::floor(31.5 * akq)) - 2; }
 struct FwdPlan {
     std::vector<int> order;
     std::vector<int> groups;  // 4 ints per group
+    int max_strips = 0;
 };
 FwdPlan forward_plan(const float* angles_deg, int na, int w, int h, int nd);
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
-                           int na, int nd, Trig trig, const int4* d_groups, int ngroups,
+                           int na, int nd, Trig trig, const int4* d_groups, int ngroups, int max_strips,
                            const int* d_order, const int4* d_box, const int2* d_band, float* d_sino,
                            cudaStream_t st);
 // Twiddle tables of the filter's FFT of length L (every radix-16 pass and the
@@ -276,7 +289,7 @@ struct ctb_ctx {
     // Forward projector plans (angle groups) per (angle set, w, h, nd).
     struct FwdPlanDev {
         ctb::DevBuf groups, order;
-        int ngroups = 0;
+        int ngroups = 0, max_strips = 0;
     };
     std::map<std::vector<long long>, FwdPlanDev> fwd_plans;
     std::vector<long long> img_border_geom;  // geometry the image borders were zeroed for

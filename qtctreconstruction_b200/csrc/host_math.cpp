@@ -236,11 +236,16 @@ namespace ctb {
 FwdPlan forward_plan(const float* angles_deg, int na, int w, int h, int nd) {
     (void)w;
     (void)h;
-    (void)nd;
     std::vector<int> lists[2];
+    std::vector<double> akq(na);
     for (int a = 0; a < na; ++a) {
-        const double th = static_cast<double>(angles_deg[a]) * 3.14159265358979323846 / 180.0;
-        lists[std::fabs(std::cos(th)) >= std::fabs(std::sin(th)) ? 0 : 1].push_back(a);
+        // the projector's own trig (k_trig): sincospi of deg / 180 in double
+        const double t = static_cast<double>(angles_deg[a]) / 180.0;
+        const double c = std::fabs(std::cos(3.14159265358979323846 * t));
+        const double s = std::fabs(std::sin(3.14159265358979323846 * t));
+        const int axis = c >= s ? 0 : 1;
+        akq[a] = axis == 0 ? c : s;
+        lists[axis].push_back(a);
     }
     FwdPlan plan;
     for (int axis = 0; axis < 2; ++axis) {
@@ -248,8 +253,17 @@ FwdPlan forward_plan(const float* angles_deg, int na, int w, int h, int nd) {
         for (size_t i = 0; i < L.size(); i += kFwdGroup) {
             const int first = static_cast<int>(plan.order.size());
             const int cnt = static_cast<int>(std::min<size_t>(kFwdGroup, L.size() - i));
-            for (int k = 0; k < cnt; ++k) plan.order.push_back(L[i + k]);
-            plan.groups.insert(plan.groups.end(), {first, cnt, axis, 0});
+            double amin = 1.0;
+            for (int k = 0; k < cnt; ++k) {
+                plan.order.push_back(L[i + k]);
+                amin = std::min(amin, akq[L[i + k]]);
+            }
+            // the device's axis test may see |cos| = |sin| the other way: the
+            // smaller coefficient is then 1/sqrt 2 to rounding, which the bin
+            // to spare in fwd_strip_bins covers
+            const int K = std::max(1, fwd_strip_bins(std::max(amin, 0.7071)));
+            plan.groups.insert(plan.groups.end(), {first, cnt, axis, K});
+            plan.max_strips = std::max(plan.max_strips, (nd + K - 1) / K);
         }
     }
     return plan;
