@@ -116,10 +116,12 @@ inline size_t fwd_plane_count(int nz) {
     return static_cast<size_t>((ng4 + kFwdPlanes - 1) / kFwdPlanes * kFwdPlanes);
 }
 // Output bins per strip for a walked-axis coefficient |kq| (>= 1/sqrt 2): the
-// 32 lanes of a warp cover bins -1/2 |kq| .. 31.5 |kq| above the strip's lower
-// edge, which must hold the strip's K bins and one bin on each side with a
-// bin to spare: K = floor(31.5 |kq|) - 2.
-inline int fwd_strip_bins(double akq) { return static_cast<int>(std::floor(31.5 * akq)) - 2; }
+// 32 lanes of a warp hold the pixels from -1/2 |kq| to 31.5 |kq| bins above the
+// strip's lower edge, which must cover the strip's K bins and the bin on
+// either side: K = floor(31.5 |kq|) - 1. (A pixel just past either end, whose
+// exact place the float arithmetic blurs by ~1e-6 bins, has a hat weight of
+// that order on the strip's outer bins.)
+inline int fwd_strip_bins(double akq) { return static_cast<int>(std::floor(31.5 * akq)) - 1; }
 struct FwdPlan {
     std::vector<int> order;
     std::vector<int> groups;  // 4 ints per group

@@ -22,8 +22,8 @@
 // m_l + 1 and m_l + 2, adding v times the hat weights of its pixel. At the
 // end of the walk the warp adds, per output bin, the accumulators of the few
 // lanes that reach it, in lane order, through shared memory. K is chosen per
-// angle group so that K + 1 <= 31.5 |kq| - 1: the lanes cover the strip's
-// bins and the half bins on both sides.
+// angle group so that K + 1 <= 31.5 |kq|: the lanes' pixels cover the
+// strip's bins and the bin on either side.
 //
 // The crossing is evaluated in double once per chunk of PCH = 16 rows (an
 // integer column plus a float offset) and stepped in float within the chunk.
@@ -312,7 +312,9 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
         const float e = static_cast<float>(PCH - 1) * f.dqf;
         const int span_lo = static_cast<int>(floorf(fminf(0.0f, e))) - 1 - (f.neg ? LANES - 1 : 0);
         const int span_hi = static_cast<int>(ceilf(fmaxf(0.0f, e))) + 2 + (f.neg ? 0 : LANES - 1);
-        for (int p0 = f.p_lo; p0 <= f.p_hi; p0 += PCH) {
+        // chunks start on multiples of PCH, so that warps whose row ranges
+        // overlap walk the same rows at about the same time
+        for (int p0 = f.p_lo & ~(PCH - 1); p0 <= f.p_hi; p0 += PCH) {
             const double qs = fma(static_cast<double>(p0), f.dq, f.q0);
             const double qfl = floor(qs);
             const int base = static_cast<int>(qfl);

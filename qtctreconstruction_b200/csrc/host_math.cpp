@@ -258,9 +258,7 @@ FwdPlan forward_plan(const float* angles_deg, int na, int w, int h, int nd) {
                 plan.order.push_back(L[i + k]);
                 amin = std::min(amin, akq[L[i + k]]);
             }
-            // the device's axis test may see |cos| = |sin| the other way: the
-            // smaller coefficient is then 1/sqrt 2 to rounding, which the bin
-            // to spare in fwd_strip_bins covers
+            // near 45 degrees the coefficient is 1/sqrt 2 to rounding
             const int K = std::max(1, fwd_strip_bins(std::max(amin, 0.7071)));
             plan.groups.insert(plan.groups.end(), {first, cnt, axis, K});
             plan.max_strips = std::max(plan.max_strips, (nd + K - 1) / K);
