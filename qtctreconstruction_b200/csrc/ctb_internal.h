@@ -102,15 +102,17 @@ constexpr int kFwdRows = 16;   // walked rows per chunk (crossing in double once
 constexpr int kFwdGroup = 4;   // angles per CTA
 constexpr int kFwdPlanes = 2;  // float4 image planes (4 slices each) per thread
 // Zero border of the normalised image planes: kFwdGuard pixels on both sides
-// of every row (a warp's 32 columns, clamped into it where the strip leaves
-// the image) and kFwdRows rows after the last, so that every chunk the
-// projector walks reads inside the plane.
-constexpr int kFwdGuard = 32;
+// of every row (the projector's windows reach at most 50 columns outside the
+// image) and kFwdRows rows after the last, so that every chunk the projector
+// walks reads inside the plane.
+constexpr int kFwdGuard = 64;
 inline size_t fwd_plane_elems(int np, int nq) {
     return static_cast<size_t>(np + kFwdRows) * static_cast<size_t>(nq + 2 * kFwdGuard);
 }
 // Float4 planes allocated for nz slices: whole groups of kFwdPlanes, since a
-// projector CTA reads all planes of its group.
+// projector CTA reads all planes of its group. The kFwdPlanes = 2 planes of a
+// pair are interleaved per pixel (two float4: 8 slices in 32 bytes), so a pair
+// occupies 2 fwd_plane_elems float4.
 inline size_t fwd_plane_count(int nz) {
     const int ng4 = (nz + 3) / 4;
     return static_cast<size_t>((ng4 + kFwdPlanes - 1) / kFwdPlanes * kFwdPlanes);

@@ -82,8 +82,10 @@ __global__ void __launch_bounds__(1024) k_slice_stats(const float* __restrict__ 
 // skip_zero = 0 every pixel is normalised, as the reference's CUDA backend does
 // (CUDABackend.cu:46-50); imgT may then be null (the ray march reads rows). Both copies
 // use the zero-bordered layout of the projector (kFwdGuard pixels left and
-// right of every row, kFwdRows rows below the last); only the interior is
-// written here, the borders are zeroed when the buffers are set up. With box
+// right of every row, kFwdRows rows below the last; a pixel holds the 8 slices
+// of a plane pair as two float4, group zg being half zg % 2 of pair zg / 2);
+// only the interior is written here, the borders are zeroed when the buffers
+// are set up. With box
 // set, box[2 zg] = {x min, x max, y min, y max} of the pixels with a non-zero
 // value in any slice of the group and box[2 zg + 1].x the largest
 // (2x - w + 1)^2 + (2y - h + 1)^2 among them (four times the squared distance
@@ -140,7 +142,7 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
             r4 = max(r4, dx * dx + dy * dy);
         }
         tile[ty + 8 * r][tx] = q;
-        if (x < w && y < h) img[(zg * rw + y) * pw + x + kFwdGuard] = q;
+        if (x < w && y < h) img[((zg / 2 * rw + y) * pw + x + kFwdGuard) * 2 + (zg & 1)] = q;
     }
     __shared__ int4 wbox[8];  // per warp, then one set of atomics per block
     __shared__ int wr4[8];
@@ -216,7 +218,7 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int x = x0 + ty + 8 * r, y = y0 + tx;
-        if (imgT && x < w && y < h) imgT[(zg * rh + x) * ph + y + kFwdGuard] = tile[tx][ty + 8 * r];
+        if (imgT && x < w && y < h) imgT[((zg / 2 * rh + x) * ph + y + kFwdGuard) * 2 + (zg & 1)] = tile[tx][ty + 8 * r];
     }
 }
 
@@ -240,7 +242,8 @@ __global__ void __launch_bounds__(128) k_raymarch(const float4* __restrict__ img
     const int zg = blockIdx.z;
     if (b >= nd) return;
     const long long pitch = w + 2 * kFwdGuard;
-    const float4* plane = img + static_cast<long long>(zg) * (h + kFwdRows) * pitch + kFwdGuard;
+    // group zg is half zg % 2 of the pixels (two float4 each) of plane pair zg / 2
+    const float4* plane = img + static_cast<long long>(zg / 2) * (h + kFwdRows) * pitch * 2 + 2 * kFwdGuard + (zg & 1);
     const double2 tc = cs[a];
     const float c = static_cast<float>(tc.x), s = static_cast<float>(tc.y);
     const float cx = 0.5f * static_cast<float>(w - 1), cy = 0.5f * static_cast<float>(h - 1);
@@ -276,9 +279,9 @@ __global__ void __launch_bounds__(128) k_raymarch(const float4* __restrict__ img
             const int x0 = static_cast<int>(xf), y0 = static_cast<int>(yf);
             const float fx = x - xf, fy = y - yf;
             const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-            const float4* r0 = plane + static_cast<long long>(y0) * pitch + x0;
-            const float4 v00 = y0 >= 0 ? r0[0] : zero, v10 = y0 >= 0 ? r0[1] : zero;
-            const float4 v01 = y0 + 1 >= 0 ? r0[pitch] : zero, v11 = y0 + 1 >= 0 ? r0[pitch + 1] : zero;
+            const float4* r0 = plane + 2 * (static_cast<long long>(y0) * pitch + x0);
+            const float4 v00 = y0 >= 0 ? r0[0] : zero, v10 = y0 >= 0 ? r0[2] : zero;
+            const float4 v01 = y0 + 1 >= 0 ? r0[2 * pitch] : zero, v11 = y0 + 1 >= 0 ? r0[2 * pitch + 2] : zero;
             const float w00 = (1.0f - fx) * (1.0f - fy), w10 = fx * (1.0f - fy);
             const float w01 = (1.0f - fx) * fy, w11 = fx * fy;
             sum.x += w00 * v00.x + w10 * v10.x + w01 * v01.x + w11 * v11.x;

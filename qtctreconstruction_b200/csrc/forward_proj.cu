@@ -16,7 +16,8 @@
 // q*(p) of its lower bin edge: lane l owns column rint(q*) + S l (S the sign
 // of ds/dq), whose offset from the crossing is u = (l - phi) |kq| in bins,
 // phi = S (rint(q*) - q*) in [-1/2, 1/2]. So every row is one coalesced load
-// of 32 neighbouring pixels (each a float4 of 4 slices), and lane l's pixel
+// of 32 neighbouring pixels (each the 8 slices of a plane pair, 32 bytes, one
+// 256-bit load per lane), and lane l's pixel
 // always falls in bin m_l or m_l + 1 of the strip, m_l = floor((l - 1/2)
 // |kq|), whatever the row: the lane keeps three accumulators, for bins m_l,
 // m_l + 1 and m_l + 2, adding v times the hat weights of its pixel. At the
@@ -48,7 +49,8 @@ constexpr int THREADS = LANES * GMAX;
 constexpr int NP = kFwdPlanes;          // float4 planes (4 slices each) per thread
 constexpr float kRound = 12582912.0f;   // 1.5 * 2^23: x + kRound rounds x to an integer
 constexpr int kRoundBits = 0x4B400000;  // bit pattern of kRound
-static_assert(kFwdGuard >= LANES, "a clamped strip must read inside the zero border");
+static_assert(kFwdGuard >= 50, "the walked windows reach 50 columns outside the image (see strip_rows)");
+static_assert(NP == 2, "a pixel holds the 8 slices of a plane pair: two float4, one 32-byte load");
 
 struct FAngle {
     double q0;   // crossing of the strip's lower edge (bin b_lo = k K - 1) at p = 0
@@ -64,6 +66,13 @@ struct FAngle {
 };
 
 __device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+// One pixel of a plane pair: 8 slices in 32 bytes (32-byte aligned), one load.
+__device__ __forceinline__ void ld_pixel(const float4* p, float4 (&v)[NP]) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(v[0].x), "=f"(v[0].y), "=f"(v[0].z), "=f"(v[0].w), "=f"(v[1].x), "=f"(v[1].y), "=f"(v[1].z),
+          "=f"(v[1].w)
+        : "l"(p));
+}
 __device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
 
 // Lane l's first bin (relative to b_lo): floor((l - 1/2) |kq|). The combine
@@ -77,27 +86,31 @@ __device__ __forceinline__ int lane_bin(int l, float akq) {
 // base + rint(A). With phi = S (rint(A) - A), lane l's pixel lies u = (l -
 // phi) |kq| bins above the edge, and y = u - m_l - 1 = cl1 - phi |kq| (cl1 =
 // l |kq| - m_l - 1) in [-1, 1] gives its hat weights for bins m_l, m_l + 1,
-// m_l + 2: max(-y, 0), 1 - |y|, max(y, 0). A strip that lies wholly outside
-// the image at some row has its start clamped into the zero border, so every
-// read stays in the plane and such rows add zeros.
+// m_l + 2: max(-y, 0), 1 - |y|, max(y, 0).
+// Reads stay inside the zero border: a walked row lies within one row of the
+// range where the strip's columns, at most 31.5 wide, come within kReach = 2
+// columns of the non-zero box (or of the image without bounds), or at most 15
+// rows beyond it (chunks start on multiples of 16), and |dq| <= 1. So the
+// window start is at least 2 + 1 + 31.5 + 0.5 + 15 = 50 columns left of the
+// box's first column and at most 2 + 1 + 0.5 + 15 = 18.5 right of its last
+// (mirrored for S < 0), and the 32-column window stays within 50 columns of
+// the image on either side: inside the kFwdGuard = 64 border, which reads as
+// zeros.
 template <int S>
-__device__ __forceinline__ void strip_rows(const float4* __restrict__ rowp, long long pofs, int pitch, int nq,
-                                           int base, float fa, float dqf, float akq, float cl1, int lane,
+__device__ __forceinline__ void strip_rows(const float4* __restrict__ rowp, int pitch, int base, float fa, float dqf, float akq, float cl1, int lane,
                                            float2 (&acc)[3][2 * NP]) {
 #pragma unroll
     for (int pp = 0; pp < PCH; ++pp) {
         const float A = fmaf(static_cast<float>(pp), dqf, fa);
         const float tr = A + kRound;
         const float rr = tr - kRound;
-        int cb = base + (__float_as_int(tr) - kRoundBits);
-        cb = S > 0 ? min(max(cb, -LANES), nq) : min(max(cb, -1), nq + LANES - 1);
+        const int cb = base + (__float_as_int(tr) - kRoundBits);
         const float y = fmaf(S > 0 ? rr - A : A - rr, akq, cl1);
         const float w0 = fmaxf(-y, 0.0f), w2 = fmaxf(y, 0.0f), w1 = 1.0f - fabsf(y);
         const float2 W0 = make_float2(w0, w0), W1 = make_float2(w1, w1), W2 = make_float2(w2, w2);
-        const float4* px = rowp + static_cast<long long>(pp) * pitch + cb + S * lane;
+        const float4* px = rowp + 2 * (static_cast<long long>(pp) * pitch + cb + S * lane);
         float4 v[NP];
-#pragma unroll
-        for (int k = 0; k < NP; ++k) v[k] = __ldg(px + k * pofs);
+        ld_pixel(px, v);
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
             acc[0][2 * k] = __ffma2_rn(W0, lo2(v[k]), acc[0][2 * k]);
@@ -118,7 +131,7 @@ __device__ __forceinline__ void strip_rows(const float4* __restrict__ rowp, long
 // [0, 1] (bin 0) or [nd-2, nd] (bin nd-1), the reference's float s being
 // much closer than that to the exact one. The lanes' sums are added by a
 // fixed shuffle tree; every lane returns the total.
-__device__ __noinline__ void edge_bin(const float4* __restrict__ plane, long long pofs, int pitch, int nq,
+__device__ __noinline__ void edge_bin(const float4* __restrict__ plane, int pitch, int nq,
                                       const FAngle& f, int b_lo, int e, int nd, int r_lo, int r_hi, bool rows,
                                       float cxf, float cyf, int lane, float2 (&sum)[2 * NP]) {
 #pragma unroll
@@ -143,10 +156,10 @@ __device__ __noinline__ void edge_bin(const float4* __restrict__ plane, long lon
             else wgt = i0 == nd - 2 ? fr : (i0 == nd - 1 ? 1.0f : 0.0f);
             if (wgt == 0.0f) continue;
             const float2 W = make_float2(wgt, wgt);
-            const float4* px = plane + static_cast<long long>(p) * pitch + c;
+            const float4* px = plane + 2 * (static_cast<long long>(p) * pitch + c);
 #pragma unroll
             for (int k = 0; k < NP; ++k) {
-                const float4 v = __ldg(px + k * pofs);
+                const float4 v = __ldg(px + k);
                 sum[2 * k] = __ffma2_rn(W, lo2(v), sum[2 * k]);
                 sum[2 * k + 1] = __ffma2_rn(W, hi2(v), sum[2 * k + 1]);
             }
@@ -191,13 +204,15 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
     constexpr double kReach = 2.0;  // margin of the row ranges (columns)
 
     // p range (within rows [rl, rh]) where crossings [qa, qb] (at p = 0) come
-    // within reach of columns [cl, ch]
-    auto prange = [&](double qa, double qb, double dq, int cl, int ch, int rl, int rh, int& lo, int& hi) {
+    // within reach of columns [cl, ch]; idq = 1 / dq (the margins of one row
+    // and kReach columns absorb its rounding)
+    auto prange = [&](double qa, double qb, double dq, double idq, int cl, int ch, int rl, int rh, int& lo,
+                      int& hi) {
         lo = rl;
         hi = rh;
         if (dq != 0.0) {
-            const double pa0 = (cl - kReach - qa) / dq, pb0 = (ch + kReach - qa) / dq;
-            const double pa1 = (cl - kReach - qb) / dq, pb1 = (ch + kReach - qb) / dq;
+            const double pa0 = (cl - kReach - qa) * idq, pb0 = (ch + kReach - qa) * idq;
+            const double pa1 = (cl - kReach - qb) * idq, pb1 = (ch + kReach - qb) * idq;
             lo = max(rl, static_cast<int>(floor(fmin(fmin(pa0, pb0), fmin(pa1, pb1)))) - 1);
             hi = min(rh, static_cast<int>(ceil(fmax(fmax(pa0, pb0), fmax(pa1, pb1)))) + 1);
         } else if (fmax(qa, qb) < cl - kReach || fmin(qa, qb) > ch + kReach) {
@@ -243,21 +258,24 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
         int e0 = 0, e1 = -1, e2 = 0, e3 = -1;
         if (ch >= cl) {  // an empty box (all slices zero) leaves no rows
             // the strip's pixels have s in (b_lo, b_lo + K + 1)
-            prange(f.q0, f.q0 + (K + 1) * f.inv, f.dq, cl, ch, rl, rh, f.p_lo, f.p_hi);
+            const double idq = f.dq != 0.0 ? 1.0 / f.dq : 0.0;
+            prange(f.q0, f.q0 + (K + 1) * f.inv, f.dq, idq, cl, ch, rl, rh, f.p_lo, f.p_hi);
             // Rows where the strip meets the disc: in the frame
             // u' = (q - cq) kq + (p - cp) kp, v = (p - cp) kq - (q - cq) kp the
             // strip is u' in [U0, U1], the disc u'^2 + v^2 <= rad^2, and p - cp
             // = u' kp + v kq. The rectangle u' in [max(U0, -rad), min(U1, rad)],
             // |v| <= sqrt(rad^2 - m^2) (m the smallest |u'| there) holds their
             // intersection.
-            const double rad = 0.5 * sqrt(static_cast<double>(r4)) + 1.5;
+            // (single-precision roots: their error, ~1e-4 pixels, is far inside
+            // the margins of 1.5 pixels and 2 rows)
+            const double rad = 0.5 * sqrtf(static_cast<float>(r4)) + 1.5;
             const double u0 = static_cast<double>(b_lo) - dcf, u1 = u0 + K + 1;
             const double a0 = fmax(fmin(u0, u1), -rad), a1 = fmin(fmax(u0, u1), rad);
             if (a0 > a1) {
                 f.p_hi = -1;
             } else {
                 const double m = (a0 <= 0.0 && a1 >= 0.0) ? 0.0 : fmin(fabs(a0), fabs(a1));
-                const double vm = sqrt(fmax(0.0, rad * rad - m * m));
+                const double vm = sqrtf(static_cast<float>(fmax(0.0, rad * rad - m * m)));
                 const double e0d = a0 * kp, e1d = a1 * kp, ev = vm * fabs(kq);
                 const int dlo = static_cast<int>(floor(cp + fmin(e0d, e1d) - ev)) - 2;
                 const int dhi = static_cast<int>(ceil(cp + fmax(e0d, e1d) + ev)) + 2;
@@ -265,9 +283,11 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
                 f.p_hi = min(f.p_hi, dhi);
             }
             // rows of the edge passes: s within [-1, 2] of bin 0, [nd-3, nd+1] of bin nd-1
-            if (has0) prange(f.q0 + (-1 - b_lo) * f.inv, f.q0 + (2 - b_lo) * f.inv, f.dq, cl, ch, rl, rh, e0, e1);
+            if (has0)
+                prange(f.q0 + (-1 - b_lo) * f.inv, f.q0 + (2 - b_lo) * f.inv, f.dq, idq, cl, ch, rl, rh, e0, e1);
             if (has_last)
-                prange(f.q0 + (nd - 3 - b_lo) * f.inv, f.q0 + (nd + 1 - b_lo) * f.inv, f.dq, cl, ch, rl, rh, e2, e3);
+                prange(f.q0 + (nd - 3 - b_lo) * f.inv, f.q0 + (nd + 1 - b_lo) * f.inv, f.dq, idq, cl, ch, rl, rh, e2,
+                       e3);
         }
         fa[tid] = f;
         erow[tid][0] = e0;
@@ -289,11 +309,11 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
     }
 
     const int pitch = nq + 2 * kFwdGuard;
-    const long long pstride = static_cast<long long>(np + PCH) * pitch;
-    // the planes are allocated in whole groups of NP: the ones past the last
-    // slice are read but their sums are not stored
-    const long long pofs = pstride;
-    const float4* plane = (rows ? img : imgT) + g0 * pstride + kFwdGuard;
+    // the CTA's plane pair: (np + PCH) rows of pitch pixels of 8 slices (two
+    // float4). Pairs are allocated whole: a half past the last slice is read
+    // but its sums are not stored
+    const long long pstride = 2LL * (np + PCH) * pitch;
+    const float4* plane = (rows ? img : imgT) + blockIdx.z * pstride + 2 * kFwdGuard;
     // 8-row bands of the walked axis: row bands (x ranges) of the group when
     // walking rows, its column bands (y ranges) when walking columns
     const int nby = (h + 7) / 8, nbx = (w + 7) / 8;
@@ -338,9 +358,9 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
             }
             // skip the chunk when the strip's columns over its rows miss them
             if (ch < cl || base + span_hi < cl || base + span_lo > ch) continue;
-            const float4* rowp = plane + static_cast<long long>(p0) * pitch;
-            if (f.neg) strip_rows<-1>(rowp, pofs, pitch, nq, base, fq, f.dqf, akq, cl1, lane, acc);
-            else strip_rows<1>(rowp, pofs, pitch, nq, base, fq, f.dqf, akq, cl1, lane, acc);
+            const float4* rowp = plane + 2LL * p0 * pitch;
+            if (f.neg) strip_rows<-1>(rowp, pitch, base, fq, f.dqf, akq, cl1, lane, acc);
+            else strip_rows<1>(rowp, pitch, base, fq, f.dqf, akq, cl1, lane, acc);
         }
 #pragma unroll
         for (int r = 0; r < 3; ++r)
@@ -382,7 +402,7 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
         if (!(side == 0 ? has0 : has_last)) continue;
         const int eb = side == 0 ? 0 : nd - 1;
         float2 sum[2 * NP];
-        edge_bin(plane, pofs, pitch, nq, f, b_lo, eb, nd, erow[ja][2 * side], erow[ja][2 * side + 1], rows, cxf,
+        edge_bin(plane, pitch, nq, f, b_lo, eb, nd, erow[ja][2 * side], erow[ja][2 * side + 1], rows, cxf,
                  cyf, lane, sum);
         if (lane == 0) {
 #pragma unroll
