@@ -22,7 +22,7 @@
 // |kq|), whatever the row: the lane keeps three accumulators, for bins m_l,
 // m_l + 1 and m_l + 2, adding v times the hat weights of its pixel. At the
 // end of the walk the warp adds, per output bin, the accumulators of the few
-// lanes that reach it, in lane order, through shared memory. K is chosen per
+// lanes that reach it, in lane order, gathered by warp shuffles. K is chosen per
 // angle group so that K + 1 <= 31.5 |kq|: the lanes' pixels cover the
 // strip's bins and the bin on either side.
 //
@@ -50,6 +50,7 @@ constexpr int NP = kFwdPlanes;          // float4 planes (4 slices each) per thr
 constexpr float kRound = 12582912.0f;   // 1.5 * 2^23: x + kRound rounds x to an integer
 constexpr int kRoundBits = 0x4B400000;  // bit pattern of kRound
 static_assert(kFwdGuard >= 50, "the walked windows reach 50 columns outside the image (see strip_rows)");
+static_assert(PCH == 16, "a chunk is two 8-row bands of the non-zero bounds");
 static_assert(NP == 2, "a pixel holds the 8 slices of a plane pair: two float4, one 32-byte load");
 
 struct FAngle {
@@ -96,11 +97,12 @@ __device__ __forceinline__ int lane_bin(int l, float akq) {
 // (mirrored for S < 0), and the 32-column window stays within 50 columns of
 // the image on either side: inside the kFwdGuard = 64 border, which reads as
 // zeros.
-template <int S>
-__device__ __forceinline__ void strip_rows(const float4* __restrict__ rowp, int pitch, int base, float fa, float dqf, float akq, float cl1, int lane,
-                                           float2 (&acc)[3][2 * NP]) {
+// Rows P0 .. P0 + NR - 1 of the chunk.
+template <int S, int P0, int NR>
+__device__ __forceinline__ void strip_rows(const float4* __restrict__ rowp, int pitch, int base, float fa,
+                                           float dqf, float akq, float cl1, int lane, float2 (&acc)[3][2 * NP]) {
 #pragma unroll
-    for (int pp = 0; pp < PCH; ++pp) {
+    for (int pp = P0; pp < P0 + NR; ++pp) {
         const float A = fmaf(static_cast<float>(pp), dqf, fa);
         const float tr = A + kRound;
         const float rr = tr - kRound;
@@ -183,7 +185,6 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
                                                         float* __restrict__ sino) {
     __shared__ FAngle fa[GMAX];
     __shared__ int erow[GMAX][4];                      // edge-pass rows: bin 0 [lo, hi], bin nd-1 [lo, hi]
-    __shared__ float2 red[GMAX][3][2 * NP][LANES];     // the lanes' accumulators, for the combine
 
     const int4 grp = groups[blockIdx.y];
     const int cnt = grp.y;
@@ -329,66 +330,84 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
         const float akq = f.akq;
         const int ml = lane_bin(lane, akq);
         const float cl1 = fmaf(static_cast<float>(lane), akq, -static_cast<float>(ml + 1));
-        const float e = static_cast<float>(PCH - 1) * f.dqf;
-        const int span_lo = static_cast<int>(floorf(fminf(0.0f, e))) - 1 - (f.neg ? LANES - 1 : 0);
-        const int span_hi = static_cast<int>(ceilf(fmaxf(0.0f, e))) + 2 + (f.neg ? 0 : LANES - 1);
         // chunks start on multiples of PCH, so that warps whose row ranges
-        // overlap walk the same rows at about the same time
+        // overlap walk the same rows at about the same time; each half of a
+        // chunk is then exactly one 8-row band
         for (int p0 = f.p_lo & ~(PCH - 1); p0 <= f.p_hi; p0 += PCH) {
             const double qs = fma(static_cast<double>(p0), f.dq, f.q0);
             const double qfl = floor(qs);
             const int base = static_cast<int>(qfl);
             const float fq = static_cast<float>(qs - qfl);
-            // the chunk's non-zero columns: the ranges of the 8-row bands its
-            // rows fall in, over the CTA's slice groups
-            int cl = f.c_lo, ch = f.c_hi;
-            if (band) {
-                cl = INT_MAX;
-                ch = -1;
-                const int b1 = min((p0 + PCH - 1) >> 3, nb_p - 1);
-                for (int k = 0; k < NP; ++k) {
-                    if (g0 + k >= ng4) break;
-                    const int2* bk = band + static_cast<long long>(g0 + k) * nb_all + nb_off;
-                    for (int bi = p0 >> 3; bi <= b1; ++bi) {
-                        const int2 r = __ldg(bk + bi);
+            // Each half walks only when the columns its lanes read, base +
+            // rint(fq + pp dqf) + S l with fq in [0, 1), meet its non-zero
+            // columns: the range of its band over the CTA's slice groups
+            // (none for rows past the image), or the box without bands. A
+            // skipped half adds only zeros.
+            bool walk[2];
+#pragma unroll
+            for (int hh = 0; hh < 2; ++hh) {
+                int cl = f.c_lo, ch = f.c_hi;
+                if (band) {
+                    cl = INT_MAX;
+                    ch = -1;
+                    const int bi = (p0 >> 3) + hh;
+                    for (int k = 0; k < NP && bi < nb_p; ++k) {
+                        if (g0 + k >= ng4) break;
+                        const int2 r = __ldg(band + static_cast<long long>(g0 + k) * nb_all + nb_off + bi);
                         cl = min(cl, r.x);
                         ch = max(ch, r.y);
                     }
                 }
+                const float e0 = static_cast<float>(8 * hh) * f.dqf, e1 = static_cast<float>(8 * hh + 7) * f.dqf;
+                const int lo = base + static_cast<int>(floorf(fminf(e0, e1))) - 1 - (f.neg ? LANES - 1 : 0);
+                const int hi = base + static_cast<int>(ceilf(fmaxf(e0, e1))) + 2 + (f.neg ? 0 : LANES - 1);
+                walk[hh] = ch >= cl && hi >= cl && lo <= ch;
             }
-            // skip the chunk when the strip's columns over its rows miss them
-            if (ch < cl || base + span_hi < cl || base + span_lo > ch) continue;
+            const bool w0 = walk[0], w1 = walk[1];
             const float4* rowp = plane + 2LL * p0 * pitch;
-            if (f.neg) strip_rows<-1>(rowp, pitch, base, fq, f.dqf, akq, cl1, lane, acc);
-            else strip_rows<1>(rowp, pitch, base, fq, f.dqf, akq, cl1, lane, acc);
+            if (f.neg) {
+                if (w0) strip_rows<-1, 0, 8>(rowp, pitch, base, fq, f.dqf, akq, cl1, lane, acc);
+                if (w1) strip_rows<-1, 8, 8>(rowp, pitch, base, fq, f.dqf, akq, cl1, lane, acc);
+            } else {
+                if (w0) strip_rows<1, 0, 8>(rowp, pitch, base, fq, f.dqf, akq, cl1, lane, acc);
+                if (w1) strip_rows<1, 8, 8>(rowp, pitch, base, fq, f.dqf, akq, cl1, lane, acc);
+            }
         }
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-            for (int j = 0; j < 2 * NP; ++j) red[ja][r][j][lane] = acc[r][j];
     }
-    __syncwarp();
     if (!has_a) return;
     const FAngle& f = fa[ja];
     const long long zst = static_cast<long long>(na) * nd;  // slice stride of the sinograms
     const long long ob = static_cast<long long>(f.a) * nd;
-    // output bin t = lane + 1 of the strip: the sum of accumulator t - m_l of
-    // every lane l with m_l in [t - 2, t], in lane order
+    // Output bin t = lane + 1 of the strip is the sum, in lane order, of
+    // accumulator t - m_l of every lane l with m_l in [t - 2, t]. Lanes with
+    // equal m_l form runs of one or two (m_l + 2 - m_l >= 2|kq| > 1) and the
+    // runs' values are -1, 0, 1, ... in lane order (consecutive m differ by at
+    // most |kq| <= 1, and m_0 = -1), so run m starts at the (m + 1)-th set bit
+    // (counting from 0) of `firsts`. The terms come by warp shuffles.
+    constexpr unsigned kAll = 0xffffffffu;
+    const int ml = lane_bin(lane, f.akq);
+    const int mprev = __shfl_up_sync(kAll, ml, 1);
+    const unsigned firsts = __ballot_sync(kAll, lane == 0 || mprev != ml);
     const int t = lane + 1;
+    float2 sum[2 * NP];
+#pragma unroll
+    for (int j = 0; j < 2 * NP; ++j) sum[j] = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int r = 2; r >= 0; --r) {
+        const unsigned l0 = __fns(firsts, 0, t - r + 2);  // first lane of run t - r (or ~0u: none)
+        const bool ok0 = l0 < LANES;
+        const bool ok1 = ok0 && l0 + 1 < LANES && !((firsts >> (l0 + 1)) & 1u);
+        const int s0 = ok0 ? static_cast<int>(l0) : lane, s1 = ok1 ? static_cast<int>(l0) + 1 : lane;
+#pragma unroll
+        for (int j = 0; j < 2 * NP; ++j) {
+            const float2 a0 = make_float2(__shfl_sync(kAll, acc[r][j].x, s0), __shfl_sync(kAll, acc[r][j].y, s0));
+            const float2 a1 = make_float2(__shfl_sync(kAll, acc[r][j].x, s1), __shfl_sync(kAll, acc[r][j].y, s1));
+            if (ok0) sum[j] = __fadd2_rn(sum[j], a0);
+            if (ok1) sum[j] = __fadd2_rn(sum[j], a1);
+        }
+    }
     const int b = b_lo + t;
     if (lane < nout && b != 0 && b != nd - 1) {
-        float2 sum[2 * NP];
-#pragma unroll
-        for (int j = 0; j < 2 * NP; ++j) sum[j] = make_float2(0.0f, 0.0f);
-        // m_l >= t - 2 needs (l - 1/2) |kq| >= t - 2: start safely below
-        for (int l = max(0, static_cast<int>(floorf(static_cast<float>(t - 2) / f.akq)) - 1); l < LANES; ++l) {
-            const int m = lane_bin(l, f.akq);
-            if (m > t) break;
-            const int r = t - m;
-            if (r > 2) continue;
-#pragma unroll
-            for (int j = 0; j < 2 * NP; ++j) sum[j] = __fadd2_rn(sum[j], red[ja][r][j][l]);
-        }
 #pragma unroll
         for (int j = 0; j < 2 * NP; ++j) {
             const int z = 4 * g0 + 2 * j;  // slices z, z + 1 of pair j
