@@ -131,12 +131,14 @@ __global__ void k_wait_selftest(unsigned limit_us, unsigned* err) {
     __syncthreads();
 }
 
+// The fields the inner loop reads every angle come first: one 16-byte
+// shared-memory broadcast per warp and angle.
 struct AngleRec {
     float f0;  // tile-origin u minus window start
     float c, s;
-    int ws;    // window start bin (unguarded coordinates)
-    float cf, sf;  // the reference's float cos/sin (edge decisions only)
     int edge;      // the window reaches a detector edge: decide taps like the reference
+    int ws;        // window start bin (unguarded coordinates)
+    float cf, sf;  // the reference's float cos/sin (edge decisions only)
     int pad;
 };
 
