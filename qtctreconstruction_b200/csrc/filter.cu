@@ -22,7 +22,9 @@
 // radix-16 Stockham transform (one
 // radix-2/4/8 pass when log2 L is not a multiple of 4) with twiddles read
 // from per-pass tables of correctly rounded values laid out so that the
-// threads of a warp read consecutive entries (fft_twiddle_table). The last
+// threads of a warp read consecutive entries (fft_twiddle_table); the packed
+// kernel reads w^1, w^2, w^3 and w^4, w^8, w^12 of a butterfly and forms the
+// other nine twiddles as one product each (tw_set). The last
 // inverse pass writes its natural-order samples straight to the output rows, float4 per bin (one
 // value per slice), the layout the backprojector stages, scaled by
 // pi/(2 na) times the slice's denormalisation span.
@@ -592,6 +594,43 @@ __device__ __forceinline__ C2 c2tw(C2 v, float4 w) {
     return INV ? c2mulc(v, cc, ss, nss) : c2mul(v, cc, ss, nss);
 }
 
+// Product of two packed twiddles {c, c, s, s}; nq = {-s, -s} of q.
+__device__ __forceinline__ float4 tw_mul(float4 p, float4 q, float2 nq) {
+    const float2 c1 = make_float2(p.x, p.y), s1 = make_float2(p.z, p.w);
+    const float2 c2 = make_float2(q.x, q.y), s2 = make_float2(q.z, q.w);
+    const float2 cc = __ffma2_rn(s1, nq, __fmul2_rn(c1, c2));
+    const float2 ss = __ffma2_rn(c1, s2, __fmul2_rn(s1, c2));
+    return make_float4(cc.x, cc.y, ss.x, ss.y);
+}
+// The twiddles w^r, r = 1 .. R-1, of one butterfly from a packed table laid out
+// r-major with stride `st` (entry (r - 1) st): w^1, w^2, w^3 and the powers
+// w^4, w^8, w^12 (radix 16; w^4 for radix 8) are read, the others formed as
+// w^(4a) w^b (a one product from two correctly rounded values, ~1.5 ulp), so
+// a pass reads 6 of its 15 table entries (4 of 7 at radix 8).
+template <int R>
+__device__ __forceinline__ void tw_set(const float4* __restrict__ t, int st, float4 (&w)[16]) {
+    w[1] = __ldg(t);
+    if constexpr (R >= 4) {
+        w[2] = __ldg(t + st);
+        w[3] = __ldg(t + 2 * st);
+    }
+    if constexpr (R >= 8) {
+        w[4] = __ldg(t + 3 * st);
+        const float2 n1 = make_float2(-w[1].z, -w[1].w), n2 = make_float2(-w[2].z, -w[2].w),
+                     n3 = make_float2(-w[3].z, -w[3].w);
+        if constexpr (R == 16) {
+            w[8] = __ldg(t + 7 * st);
+            w[12] = __ldg(t + 11 * st);
+        }
+#pragma unroll
+        for (int a = 4; a < R; a += 4) {
+            w[a + 1] = tw_mul(w[a], w[1], n1);
+            w[a + 2] = tw_mul(w[a], w[2], n2);
+            w[a + 3] = tw_mul(w[a], w[3], n3);
+        }
+    }
+}
+
 // One radix-16 Stockham pass (Ns > 1) of length L by T = L/16 threads.
 template <int L, int NS, bool INV>
 __device__ __forceinline__ void pass16p(float4* buf, int j, const float4* __restrict__ tw4) {
@@ -600,9 +639,10 @@ __device__ __forceinline__ void pass16p(float4* buf, int j, const float4* __rest
     C2 v[16];
 #pragma unroll
     for (int r = 0; r < 16; ++r) v[r] = ld_c2(buf, j + r * LR);
-    const float4* t = tw4 + 15 * (NS - 1) + k;
+    float4 w[16];
+    tw_set<16>(tw4 + 15 * (NS - 1) + k, NS, w);
 #pragma unroll
-    for (int r = 1; r < 16; ++r) v[r] = c2tw<INV>(v[r], __ldg(t + (r - 1) * NS));
+    for (int r = 1; r < 16; ++r) v[r] = c2tw<INV>(v[r], w[r]);
     dftp<16, INV>(v);
     __syncthreads();
     const int base = (j - k) * 16 + k;
@@ -686,9 +726,10 @@ __global__ void __launch_bounds__((1 << LOGL) / 16, 4) k_filter4(const __grid_co
 #pragma unroll
         for (int r = 0; r < 16; ++r) v[r] = ld_c2(smem4, j + r * LR);
         if constexpr (LR > 1) {
-            const float4* t = tw4 + 15 * (LR - 1) + j;
+            float4 w[16];
+            tw_set<16>(tw4 + 15 * (LR - 1) + j, LR, w);
 #pragma unroll
-            for (int r = 1; r < 16; ++r) v[r] = c2tw<false>(v[r], __ldg(t + (r - 1) * LR));
+            for (int r = 1; r < 16; ++r) v[r] = c2tw<false>(v[r], w[r]);
         }
         dftp<16, false>(v);
 #pragma unroll
@@ -722,9 +763,10 @@ __global__ void __launch_bounds__((1 << LOGL) / 16, 4) k_filter4(const __grid_co
 #pragma unroll
             for (int r = 0; r < R0; ++r) v[r] = ld_c2(smem4, j + r * LR);
             if constexpr (LR > 1) {
-                const float4* t = tw4 + (R0 == 16 ? 15 * (LR - 1) : 15 * (L / 8 - 1)) + j;
+                float4 w[16];
+                tw_set<R0>(tw4 + (R0 == 16 ? 15 * (LR - 1) : 15 * (L / 8 - 1)) + j, LR, w);
 #pragma unroll
-                for (int r = 1; r < R0; ++r) v[r] = c2tw<true>(v[r], __ldg(t + (r - 1) * LR));
+                for (int r = 1; r < R0; ++r) v[r] = c2tw<true>(v[r], w[r]);
             }
             dftp<R0, true>(v);
 #pragma unroll
