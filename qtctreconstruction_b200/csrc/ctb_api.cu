@@ -359,7 +359,7 @@ ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins
 // Slabs of a host-buffer pipeline: {first slice, slices}, whole 8-slice
 // groups (the forward projector's groups, and whole 4-slice groups of the
 // filter and backprojector, so that a slab-streamed result equals one pass
-// over the whole stack bit for bit), about depth/8 slices each. The host->device
+// over the whole stack bit for bit), about depth/16 slices each. The host->device
 // copy of slab k + 1 and the device->host copy of slab k - 1 run on their own
 // streams while slab k is computed. The schedule tapers at both ends (a
 // quarter slab, three quarters, double slabs, three quarters, a quarter), so
@@ -368,7 +368,7 @@ ctb_status fbp_stage(ctb_ctx* ctx, const float* d_sino, int nz, int na, int bins
 // enough to keep their tail waves small; each copy in stays shorter than the
 // slab computed beside it.
 std::vector<int2> plan_slabs(int depth) {
-    constexpr int kSlabs = 8;
+    constexpr int kSlabs = 16;
     std::vector<int2> slabs;
     if (depth <= 16) {
         slabs.push_back(make_int2(0, depth));

@@ -205,6 +205,31 @@ __device__ __forceinline__ float2 twiddle_mul(float2 v, float2 w) {
     return INV ? cmulc(v, w) : cmul(v, w);
 }
 
+// The twiddles w^r, r = 1 .. R-1, of one butterfly from a table laid out
+// r-major with stride `st`: w^1, w^2, w^3 and w^4, w^8, w^12 (radix 16; w^4
+// for radix 8) are read, the others formed as w^(4a) w^b, one product each.
+template <int R>
+__device__ __forceinline__ void tw_set_s(const float2* __restrict__ t, int st, float2 (&w)[16]) {
+    w[1] = __ldg(t);
+    if constexpr (R >= 4) {
+        w[2] = __ldg(t + st);
+        w[3] = __ldg(t + 2 * st);
+    }
+    if constexpr (R >= 8) {
+        w[4] = __ldg(t + 3 * st);
+        if constexpr (R == 16) {
+            w[8] = __ldg(t + 7 * st);
+            w[12] = __ldg(t + 11 * st);
+        }
+#pragma unroll
+        for (int a = 4; a < R; a += 4) {
+            w[a + 1] = cmul(w[a], w[1]);
+            w[a + 2] = cmul(w[a], w[2]);
+            w[a + 3] = cmul(w[a], w[3]);
+        }
+    }
+}
+
 // One Stockham pass of radix R over a length-L sequence in shared memory,
 // executed by T = L/(16 K) threads (16 K / R butterflies each). Ns is the
 // length of the sub-transforms already combined; tw holds the twiddle tables.
@@ -222,9 +247,10 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int L, int Ns, int ti
         for (int r = 0; r < R; ++r) v[bi][r] = buf[padi(j + r * LR)];
         if (Ns > 1) {
             static_assert(R == 16, "inner passes are radix 16");
-            const float2* t = tw + tw16_offset(Ns) + k;
+            float2 w[16];
+            tw_set_s<16>(tw + tw16_offset(Ns) + k, Ns, w);
 #pragma unroll
-            for (int r = 1; r < 16; ++r) v[bi][r] = twiddle_mul<INV>(v[bi][r], __ldg(t + (r - 1) * Ns));
+            for (int r = 1; r < 16; ++r) v[bi][r] = twiddle_mul<INV>(v[bi][r], w[r]);
         }
         dft<R, INV>(v[bi]);
     }
@@ -263,9 +289,10 @@ __device__ __forceinline__ void last_pass_out(const float2* buf, int L, int tid,
 #pragma unroll
         for (int r = 0; r < R; ++r) v[bi][r] = buf[padi(j + r * LR)];
         if (LR > 1) {
-            const float2* t = tw + (R == 16 ? tw16_offset(LR) : twr_offset(L)) + j;
+            float2 w[16];
+            tw_set_s<R>(tw + (R == 16 ? tw16_offset(LR) : twr_offset(L)) + j, LR, w);
 #pragma unroll
-            for (int r = 1; r < R; ++r) v[bi][r] = cmulc(v[bi][r], __ldg(t + (r - 1) * LR));
+            for (int r = 1; r < R; ++r) v[bi][r] = cmulc(v[bi][r], w[r]);
         }
         dft<R, true>(v[bi]);
         // sq = ceil(sqrt2 nd) and Lc >= sq + nd - 1 give sq <= 0.586 Lc + 1, so
@@ -329,9 +356,10 @@ __device__ __forceinline__ void fused_middle(float2* buf, int L, int tid, int T,
 #pragma unroll
         for (int r = 0; r < 16; ++r) v[bi][r] = buf[padi(j + r * LR)];
         if (LR > 1) {
-            const float2* t = tw + tw16_offset(LR) + j;
+            float2 w[16];
+            tw_set_s<16>(tw + tw16_offset(LR) + j, LR, w);
 #pragma unroll
-            for (int r = 1; r < 16; ++r) v[bi][r] = cmul(v[bi][r], __ldg(t + (r - 1) * LR));
+            for (int r = 1; r < 16; ++r) v[bi][r] = cmul(v[bi][r], w[r]);
         }
         dft16<false>(v[bi]);
 #pragma unroll
