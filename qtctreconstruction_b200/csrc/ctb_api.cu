@@ -168,7 +168,7 @@ void mark(ctb_ctx* ctx, cudaEvent_t* ev, int k) {
 // Angle groups of the forward projector for this geometry (cached; explicit
 // angle lists are keyed by their upload generation).
 ctb_status forward_plan_dev(ctb_ctx* ctx, const float* angles_deg, int na, int w, int h, int nd,
-                            const ctb_ctx::FwdPlanDev** out) {
+                            const Trig& trig, const ctb_ctx::FwdPlanDev** out) {
     const std::vector<long long> key = {angles_deg ? ctx->user_angles_gen : -1, na, w, h, nd};
     auto it = ctx->fwd_plans.find(key);
     if (it == ctx->fwd_plans.end()) {
@@ -187,6 +187,11 @@ ctb_status forward_plan_dev(ctb_ctx* ctx, const float* angles_deg, int na, int w
                                  cudaMemcpyHostToDevice));
         CTB_CUDA(ctx, cudaMemcpy(d.order.ptr, plan.order.data(), sizeof(int) * plan.order.size(),
                                  cudaMemcpyHostToDevice));
+        CTB_CUDA(ctx, cudaMalloc(&d.rec.ptr, sizeof(FwdAngleRec) * plan.order.size()));
+        // the records come from this angle generation's table (the plan's key)
+        CTB_LAUNCH(ctx, launch_fwd_angles(static_cast<const int4*>(d.groups.ptr), d.ngroups,
+                                          static_cast<const int*>(d.order.ptr), trig,
+                                          static_cast<FwdAngleRec*>(d.rec.ptr), ctx->stream));
         it = ctx->fwd_plans.emplace(key, d).first;
     }
     *out = &it->second;
@@ -236,10 +241,10 @@ ctb_status forward_stage(ctb_ctx* ctx, const float* d_vol, int w, int h, int nz,
     CTB_LAUNCH(ctx, launch_normalize(d_vol, w, h, nz, d_stats, d_img, d_imgT, ctx->stream, 1, box, band));
     mark(ctx, ev, 1);
     const ctb_ctx::FwdPlanDev* plan = nullptr;
-    CTB_TRY(forward_plan_dev(ctx, angles_deg, na, w, h, nd, &plan));
-    CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd, trig,
+    CTB_TRY(forward_plan_dev(ctx, angles_deg, na, w, h, nd, trig, &plan));
+    CTB_LAUNCH(ctx, launch_forward(d_img, d_imgT, w, h, nz, na, nd,
                                    static_cast<const int4*>(plan->groups.ptr), plan->ngroups, plan->max_strips,
-                                   static_cast<const int*>(plan->order.ptr), box, band, d_sino,
+                                   static_cast<const FwdAngleRec*>(plan->rec.ptr), box, band, d_sino,
                                    ctx->stream));
     return CTB_OK;
 }
@@ -579,6 +584,7 @@ void ctb_destroy(ctb_ctx* ctx) {
         for (auto& kv : ctx->fwd_plans) {
             cudaFree(kv.second.groups.ptr);
             cudaFree(kv.second.order.ptr);
+            cudaFree(kv.second.rec.ptr);
         }
         for (auto& e : ctx->prof_ev)
             if (e) cudaEventDestroy(e);

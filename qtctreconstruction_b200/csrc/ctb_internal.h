@@ -130,9 +130,23 @@ struct FwdPlan {
     int max_strips = 0;
 };
 FwdPlan forward_plan(const float* angles_deg, int na, int w, int h, int nd);
+// Per-angle constants of the forward projector, in plan order (slot i holds
+// angle order[i], walked along its group's axis): kq and kp, the coefficients
+// of the gathered and the walked axis, inv = 1 / kq, idq = 1 / dq with
+// dq = -kp inv (0 when kp = 0), the reference's float (cos, sin) and the angle
+// index. Computed once per plan from the angle table, so the projector's
+// per-CTA set-up reads one record instead of the order and trig tables and
+// divides nothing.
+struct FwdAngleRec {
+    double kq, kp, inv, idq;
+    float cf, sf;
+    int a, pad;
+};
+cudaError_t launch_fwd_angles(const int4* d_groups, int ngroups, const int* d_order, Trig trig,
+                              FwdAngleRec* d_rec, cudaStream_t st);
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
-                           int na, int nd, Trig trig, const int4* d_groups, int ngroups, int max_strips,
-                           const int* d_order, const int4* d_box, const int2* d_band, float* d_sino,
+                           int na, int nd, const int4* d_groups, int ngroups, int max_strips,
+                           const FwdAngleRec* d_rec, const int4* d_box, const int2* d_band, float* d_sino,
                            cudaStream_t st);
 // Twiddle tables of the filter's FFT of length L (every radix-16 pass and the
 // radix-2/4/8 last pass, r-major per pass), correctly rounded from double
@@ -292,7 +306,7 @@ struct ctb_ctx {
     long long user_angles_gen = 0;  // bumps whenever the explicit angle list changes
     // Forward projector plans (angle groups) per (angle set, w, h, nd).
     struct FwdPlanDev {
-        ctb::DevBuf groups, order;
+        ctb::DevBuf groups, order, rec;  // rec: FwdAngleRec per plan slot
         int ngroups = 0, max_strips = 0;
     };
     std::map<std::vector<long long>, FwdPlanDev> fwd_plans;

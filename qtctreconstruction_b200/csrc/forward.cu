@@ -102,8 +102,11 @@ __global__ void __launch_bounds__(256) k_normalize(const float* __restrict__ vol
     const long long pw = w + 2 * kFwdGuard, ph = h + 2 * kFwdGuard;  // row pitches
     const long long rw = h + kFwdRows, rh = w + kFwdRows;             // rows per plane
     __shared__ float4 tile[32][33];
-    const int zg = blockIdx.z;
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    // the two 4-slice groups of a plane pair run in neighbouring blocks, so
+    // both halves of each 32-byte pixel are written at about the same time
+    const int zg = 2 * blockIdx.z + (blockIdx.x & 1);
+    if (zg >= (nz + 3) / 4) return;  // a pair with one group (uniform per block)
+    const int x0 = (blockIdx.x >> 1) * 32, y0 = blockIdx.y * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
     float lo[4], inv[4];
     bool live[4];
@@ -321,7 +324,7 @@ cudaError_t launch_slice_stats(const float* d_vol, long long npx, int nz, float4
 cudaError_t launch_normalize(const float* d_vol, int w, int h, int nz, const float4* d_stats,
                              float4* d_img, float4* d_imgT, cudaStream_t st, int skip_zero,
                              int4* d_box, int2* d_band) {
-    const dim3 grid((w + 31) / 32, (h + 31) / 32, (nz + 3) / 4);
+    const dim3 grid(2 * ((w + 31) / 32), (h + 31) / 32, (nz + 7) / 8);
     k_normalize<<<grid, 256, 0, st>>>(d_vol, w, h, nz, d_stats, d_img, d_imgT, skip_zero, d_box, d_band);
     return cudaGetLastError();
 }

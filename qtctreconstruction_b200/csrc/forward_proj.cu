@@ -177,9 +177,9 @@ __device__ __noinline__ void edge_bin(const float4* __restrict__ plane, int pitc
 
 __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict__ img,
                                                         const float4* __restrict__ imgT, int w,
-                                                        int h, int nz, int na, int nd, Trig trig,
+                                                        int h, int nz, int na, int nd,
                                                         const int4* __restrict__ groups,
-                                                        const int* __restrict__ order,
+                                                        const FwdAngleRec* __restrict__ arec,
                                                         const int4* __restrict__ box,
                                                         const int2* __restrict__ band,
                                                         float* __restrict__ sino) {
@@ -236,21 +236,20 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
         }
         const int rl = rows ? bx.z : bx.x, rh = rows ? bx.w : bx.y;
         const int cl = rows ? bx.x : bx.z, ch = rows ? bx.y : bx.w;
-        const int a = order[grp.x + tid];
-        const double2 tc = trig.cs[a];
-        const double kq = rows ? tc.x : tc.y;
-        const double kp = rows ? tc.y : tc.x;
+        const FwdAngleRec R = arec[grp.x + tid];
+        const int a = R.a;
+        const double kq = R.kq;
+        const double kp = R.kp;
         // s(q, p) = (q - cq) kq + (p - cp) kp + dcf = b  <=>  q = q0(b) + p dq
         FAngle f;
-        f.inv = 1.0 / kq;
+        f.inv = R.inv;
         f.dq = -kp * f.inv;
         f.q0 = cq + (static_cast<double>(b_lo) - dcf + cp * kp) * f.inv;
         f.dqf = static_cast<float>(f.dq);
         f.akq = static_cast<float>(fabs(kq));
         f.neg = kq < 0.0 ? 1 : 0;
-        const float2 tf = trig.csf[a];
-        f.cf = tf.x;
-        f.sf = tf.y;
+        f.cf = R.cf;
+        f.sf = R.sf;
         f.a = a;
         f.c_lo = cl;
         f.c_hi = ch;
@@ -259,7 +258,7 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
         int e0 = 0, e1 = -1, e2 = 0, e3 = -1;
         if (ch >= cl) {  // an empty box (all slices zero) leaves no rows
             // the strip's pixels have s in (b_lo, b_lo + K + 1)
-            const double idq = f.dq != 0.0 ? 1.0 / f.dq : 0.0;
+            const double idq = R.idq;
             prange(f.q0, f.q0 + (K + 1) * f.inv, f.dq, idq, cl, ch, rl, rh, f.p_lo, f.p_hi);
             // Rows where the strip meets the disc: in the frame
             // u' = (q - cq) kq + (p - cp) kp, v = (p - cp) kq - (q - cq) kp the
@@ -434,15 +433,47 @@ __global__ void __launch_bounds__(THREADS, 7) k_forward(const float4* __restrict
     }
 }
 
+// One thread per angle group: the per-angle constants of its angles (the
+// expressions the projector's set-up evaluated itself before).
+__global__ void k_fwd_angles(const int4* __restrict__ groups, int ngroups, const int* __restrict__ order,
+                             Trig trig, FwdAngleRec* __restrict__ rec) {
+    const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= ngroups) return;
+    const int4 grp = groups[gi];
+    const bool rows = grp.z == 0;
+    for (int k = 0; k < grp.y; ++k) {
+        const int a = order[grp.x + k];
+        const double2 tc = trig.cs[a];
+        FwdAngleRec r;
+        r.kq = rows ? tc.x : tc.y;
+        r.kp = rows ? tc.y : tc.x;
+        r.inv = 1.0 / r.kq;
+        const double dq = -r.kp * r.inv;
+        r.idq = dq != 0.0 ? 1.0 / dq : 0.0;
+        const float2 tf = trig.csf[a];
+        r.cf = tf.x;
+        r.sf = tf.y;
+        r.a = a;
+        r.pad = 0;
+        rec[grp.x + k] = r;
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_forward(const float4* d_img, const float4* d_imgT, int w, int h, int nz,
-                           int na, int nd, Trig trig, const int4* d_groups, int ngroups, int max_strips,
-                           const int* d_order, const int4* d_box, const int2* d_band, float* d_sino,
+                           int na, int nd, const int4* d_groups, int ngroups, int max_strips,
+                           const FwdAngleRec* d_rec, const int4* d_box, const int2* d_band, float* d_sino,
                            cudaStream_t st) {
     const dim3 grid(max_strips, ngroups, ((nz + 3) / 4 + NP - 1) / NP);
-    k_forward<<<grid, dim3(LANES, GMAX), 0, st>>>(d_img, d_imgT, w, h, nz, na, nd, trig, d_groups, d_order,
-                                                  d_box, d_band, d_sino);
+    k_forward<<<grid, dim3(LANES, GMAX), 0, st>>>(d_img, d_imgT, w, h, nz, na, nd, d_groups, d_rec, d_box,
+                                                  d_band, d_sino);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fwd_angles(const int4* d_groups, int ngroups, const int* d_order, Trig trig,
+                              FwdAngleRec* d_rec, cudaStream_t st) {
+    k_fwd_angles<<<(ngroups + 127) / 128, 128, 0, st>>>(d_groups, ngroups, d_order, trig, d_rec);
     return cudaGetLastError();
 }
 
