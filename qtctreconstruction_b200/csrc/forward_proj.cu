@@ -27,10 +27,13 @@
 // strip's bins and the bin on either side.
 //
 // The crossing is evaluated in double once per chunk of PCH = 16 rows (an
-// integer column plus a float offset) and stepped in float within the chunk.
-// The warps of a CTA are the up to GMAX = 4 angles of a group that share the
-// walked axis, on the same strip index; they walk the same rows at nearly the
-// same columns and share the L1 lines. Warps never wait on one another.
+// integer column plus a float offset) and stepped in float within the chunk;
+// each 8-row half of a chunk is walked only where its lanes' columns meet the
+// non-zero pixels of that 8-row band. The warps of a CTA are the up to GMAX =
+// 4 angles of a group that share the walked axis, on the same strip index;
+// after one barrier that ends the set-up (per-angle constants from the plan's
+// FwdAngleRec table) they walk the same rows at nearly the same columns and
+// share the L1 lines, and never wait on one another again.
 // Bins 0 and nd-1 are recomputed by the warp whose strip holds them, with one
 // lane per row deciding on the reference's own float s for the few pixels
 // around those bins.
