@@ -181,6 +181,17 @@ ctb_status forward_plan_dev(ctb_ctx* ctx, const float* angles_deg, int na, int w
         ctb_ctx::FwdPlanDev d;
         d.ngroups = static_cast<int>(plan.groups.size() / 4);
         d.max_strips = plan.max_strips;
+        // frees the plan's buffers on an early exit, before the cache owns them
+        struct Pending {
+            ctb_ctx::FwdPlanDev* p;
+            ~Pending() {
+                if (p) {
+                    cudaFree(p->groups.ptr);
+                    cudaFree(p->order.ptr);
+                    cudaFree(p->rec.ptr);
+                }
+            }
+        } pending{&d};
         CTB_CUDA(ctx, cudaMalloc(&d.groups.ptr, sizeof(int) * plan.groups.size()));
         CTB_CUDA(ctx, cudaMalloc(&d.order.ptr, sizeof(int) * plan.order.size()));
         CTB_CUDA(ctx, cudaMemcpy(d.groups.ptr, plan.groups.data(), sizeof(int) * plan.groups.size(),
@@ -193,6 +204,7 @@ ctb_status forward_plan_dev(ctb_ctx* ctx, const float* angles_deg, int na, int w
                                           static_cast<const int*>(d.order.ptr), trig,
                                           static_cast<FwdAngleRec*>(d.rec.ptr), ctx->stream));
         it = ctx->fwd_plans.emplace(key, d).first;
+        pending.p = nullptr;
     }
     *out = &it->second;
     return CTB_OK;
