@@ -102,13 +102,14 @@ ACC_GATE = {"rel_l2": 1e-5, "max_abs": 1e-4}
 
 
 def accuracy_slices(nz: int, n: int):
-    """Slices whose output is checked: both sides of the 8-slice group and
-    slab boundaries of the host pipeline's schedule, the middle and the ends
-    (fewer at n >= 1024, where one FP64 slice takes seconds)."""
+    """Slices whose output is checked: both sides of the first and last slab
+    boundaries of the host pipeline's schedule (8, 24, 64, ..., 64, 24, 8
+    slices at 512), which are 8-slice group boundaries too, the middle and the
+    ends (fewer at n >= 1024, where one FP64 slice takes seconds)."""
     if n >= 1024:
         zs = [0, 15, 16, nz // 2 - 1, nz // 2, nz - 1]
     else:
-        zs = [0, 15, 16, 63, 64, nz // 2 - 1, nz // 2, nz - 65, nz - 64, nz - 1]
+        zs = [0, 7, 8, 31, 32, 95, 96, nz // 2 - 1, nz // 2, nz - 33, nz - 32, nz - 9, nz - 8, nz - 1]
     return sorted({z for z in zs if 0 <= z < nz})
 
 
