@@ -160,9 +160,9 @@ ctb_status ctb_set_convention(ctb_ctx* ctx, int convention);
 /* Forward projector bounds (SerialBackend convention; on by default). The
  * reference skips background pixels (SerialBackend.cpp:104-106). Here every
  * pixel whose normalised value is zero is an exact zero contribution, so the
- * projector walks each 8-slice group only where its detector intervals meet
- * the bounding box, the centred disc and the per-8-row-band column ranges of
- * the group's non-zero pixels.
+ * projector walks each 8-slice group only where its strips of detector bins
+ * meet the bounding box, the centred disc and the per-8-row-band column ranges
+ * of the group's non-zero pixels.
  * enable = 0 walks the whole image (same results; for timing comparisons). */
 ctb_status ctb_set_forward_bounds(ctb_ctx* ctx, int enable);
 
