@@ -550,6 +550,9 @@ def run_ours(args, cfg, rank: int, world: int, local: int):
                          "backproject": stages[3]},
             "fbp_only": {"value": updates / ((stages[2] + stages[3]) * 1e-3), "unit": UNIT,
                          "note": "filter + backprojection kernels only"},
+            "forward_only": {"value": updates / ((stages[0] + stages[1]) * 1e-3), "unit": UNIT,
+                             "note": "statistics, normalisation and forward projection only (N^2 slices angles "
+                                     "pixel-angle updates)"},
             "roofline": roof_main,
             "roofline_" + roof_other["kernel"][2:]: roof_other,
             "roofline_phantom": {"kernel": "k_phantom_sum", "bound": "hbm",
