@@ -50,6 +50,17 @@ namespace ctb {
 // float2 holding the reference's float cos/sin of degToRad(deg)
 // (SerialBackend.cpp:92-95, 198-204; Utils.cpp:44-46), computed here on the
 // host with the same libm calls.
+// A table upload from pageable host memory, complete on return. A plain
+// cudaMemcpy from pageable memory may return before its DMA has landed and is
+// ordered only against the legacy default stream, while the kernels run on
+// non-blocking streams; the copy is therefore queued on the context's stream
+// and waited for.
+ctb_status upload(ctb_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    CTB_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return CTB_OK;
+}
+
 ctb_status fill_trig(ctb_ctx* ctx, const float* angles_deg, int na, void* table) {
     std::vector<float2> csf(na);
     for (int a = 0; a < na; ++a) {
@@ -59,9 +70,8 @@ ctb_status fill_trig(ctb_ctx* ctx, const float* angles_deg, int na, void* table)
     float* d_deg = static_cast<float*>(workspace(ctx, "angles_upload", sizeof(float) * na));
     if (!d_deg) return fail(ctx, CTB_ERR_OOM, "angle upload buffer");
     CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // previous users of the buffers are done
-    CTB_CUDA(ctx, cudaMemcpy(d_deg, angles_deg, sizeof(float) * na, cudaMemcpyHostToDevice));
-    CTB_CUDA(ctx, cudaMemcpy(static_cast<double2*>(table) + na, csf.data(), sizeof(float2) * na,
-                             cudaMemcpyHostToDevice));
+    CTB_TRY(upload(ctx, d_deg, angles_deg, sizeof(float) * na));
+    CTB_TRY(upload(ctx, static_cast<double2*>(table) + na, csf.data(), sizeof(float2) * na));
     CTB_LAUNCH(ctx, launch_trig(d_deg, na, static_cast<double2*>(table), ctx->stream));
     CTB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return CTB_OK;
@@ -112,7 +122,7 @@ ctb_status filter_tables(ctb_ctx* ctx, const PadGeom& g, int type, const float2*
         DevBuf b;
         CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float2) * Hc.size()));
         b.bytes = sizeof(float2) * Hc.size();
-        CTB_CUDA(ctx, cudaMemcpy(b.ptr, Hc.data(), b.bytes, cudaMemcpyHostToDevice));
+        CTB_TRY(upload(ctx, b.ptr, Hc.data(), b.bytes));
         it = ctx->filters.emplace(key, b).first;
     }
     auto jt = ctx->twiddles.find(Lc);
@@ -121,7 +131,7 @@ ctb_status filter_tables(ctb_ctx* ctx, const PadGeom& g, int type, const float2*
         DevBuf b;
         CTB_CUDA(ctx, cudaMalloc(&b.ptr, sizeof(float2) * tw.size()));
         b.bytes = sizeof(float2) * tw.size();
-        CTB_CUDA(ctx, cudaMemcpy(b.ptr, tw.data(), b.bytes, cudaMemcpyHostToDevice));
+        CTB_TRY(upload(ctx, b.ptr, tw.data(), b.bytes));
         jt = ctx->twiddles.emplace(Lc, b).first;
     }
     *d_Hc = static_cast<const float2*>(it->second.ptr);
@@ -194,10 +204,8 @@ ctb_status forward_plan_dev(ctb_ctx* ctx, const float* angles_deg, int na, int w
         } pending{&d};
         CTB_CUDA(ctx, cudaMalloc(&d.groups.ptr, sizeof(int) * plan.groups.size()));
         CTB_CUDA(ctx, cudaMalloc(&d.order.ptr, sizeof(int) * plan.order.size()));
-        CTB_CUDA(ctx, cudaMemcpy(d.groups.ptr, plan.groups.data(), sizeof(int) * plan.groups.size(),
-                                 cudaMemcpyHostToDevice));
-        CTB_CUDA(ctx, cudaMemcpy(d.order.ptr, plan.order.data(), sizeof(int) * plan.order.size(),
-                                 cudaMemcpyHostToDevice));
+        CTB_TRY(upload(ctx, d.groups.ptr, plan.groups.data(), sizeof(int) * plan.groups.size()));
+        CTB_TRY(upload(ctx, d.order.ptr, plan.order.data(), sizeof(int) * plan.order.size()));
         CTB_CUDA(ctx, cudaMalloc(&d.rec.ptr, sizeof(FwdAngleRec) * plan.order.size()));
         // the records come from this angle generation's table (the plan's key)
         CTB_LAUNCH(ctx, launch_fwd_angles(static_cast<const int4*>(d.groups.ptr), d.ngroups,

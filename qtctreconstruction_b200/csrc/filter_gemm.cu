@@ -397,6 +397,9 @@ cudaError_t make_gemm_table(const PadGeom& g, int type, bool keep_nyquist, GemmT
     cudaError_t e = cudaMalloc(&p, NTERMS * bytes);
     if (e != cudaSuccess) return e;
     e = cudaMemcpy(p, tt.data(), NTERMS * bytes, cudaMemcpyHostToDevice);
+    // a copy from pageable memory may return before its DMA lands; the kernels
+    // that read the table run on other streams, so wait for it here
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     for (int a = 0; a < NTERMS && e == cudaSuccess; ++a)
         if (!encode_map(out->map[a], static_cast<char*>(p) + a * bytes, nrows, kpad, bn)) e = cudaErrorNotSupported;
     if (e != cudaSuccess) {
