@@ -84,3 +84,13 @@ def test_reference_arm_loads_no_product_library():
     import json
     d = json.loads(line)
     assert d["impl"] == "reference" and d["value"] > 0
+
+
+def test_accuracy_slices_straddle_the_host_schedule_ends():
+    """The bench's FP64 check covers both sides of the first and last slab
+    boundaries of the 512-slice host schedule (8, 24, 7 x 64, 24, 8)."""
+    zs = bench.accuracy_slices(512, 512)
+    for b in (8, 32, 96, 480, 504):
+        assert b - 1 in zs and b in zs, b
+    assert 0 in zs and 511 in zs and 255 in zs and 256 in zs
+    assert zs == sorted(set(zs)) and all(0 <= z < 512 for z in zs)
